@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Throughput of the twist-mesh pipeline on B200: k-point eigensolves/s.
+
+Workload (the hlm configuration the metric is quoted on): Hofstadter lattice 48 x 16 sites,
+flux 1/3 (Q=3), projected onto subband 0 (n_phi = 256, so every k-point is a 256 x 256
+complex Hermitian eigenproblem), twist mesh g=32 (theta_1 in [0,32], theta_2 in [0,32):
+1056 k-points per sample), 64 disorder samples per step = 67,584 eigensolves plus the
+projection and the Chern step.  On-site disorder is uniform in [-1,1) from the seeded
+MT19937 stream of the reference's hlm driver (seed 1 + rank).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+value : device-resident inputs, one rlmb_hlm_mesh_solve_device call per step.
+e2e   : the host-buffer C-ABI call rlmb_hlm_mesh_solve (potentials H2D, energies and
+        Chern numbers D2H inside the timed region).
+--impl reference : the reference's own CPU implementation (oracle/_ref, compiled from the
+        reference sources) on this host's cores, one theta_1 line per step.
+Multi-GPU (torchrun): every rank solves its own 64 samples (weak scaling, no data-path
+collective); the step time is the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "random-landau-model_b200")
+for _p in (REPO, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "k-point eigensolves/s & samples/hr, mixed-refined vs FP64 GPU; Chern ints exact"
+UNIT = "k-point eigensolves/s"
+LX, LY, Q, BAND, G, NS, SEED = 48, 16, 3, 0, 32, 64, 1
+N_PHI = LX * LY // Q
+N_SITES = LX * LY
+KPTS = (G + 1) * G
+SOLVES_PER_STEP = NS * KPTS
+
+
+def _config(extra=None):
+    c = {"workload": f"hlm {LX}x{LY} sites, flux 1/{Q}, band {BAND}, n_phi={N_PHI}, g={G} "
+                     f"({KPTS} k-points/sample), {NS} samples/step, seed {SEED}+rank",
+         "n_phi": N_PHI, "n_mesh": G, "samples_per_step": NS, "solves_per_step": SOLVES_PER_STEP,
+         "precision": "fp64 (complex128) eigensolve, FP64 phase accumulation",
+         "l2": "working set per step >> 126 MB L2 (each sample's 1056 matrices are 1.1 GB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for nm, v in zip(names, r[4:8]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------- reference arm (CPU)
+def _ref_hlm_lib():
+    path = os.path.join(REPO, "oracle", "_ref", "libref_hlm.so")
+    if not os.path.exists(path):
+        return None, f"{path} not built (make -C oracle needs the reference sources)"
+    lib = ctypes.CDLL(path)
+    lib.ref_hlm_solve_line.restype = None
+    lib.ref_peer_cal_chern.restype = None
+    lib.ref_hlm_potentials.restype = None
+    return lib, None
+
+
+def _ref_line_runner(threads):
+    """Closure running one theta_1 line of the reference hlm path (projection + heevd +
+    back-transform for 32 k-points, then the FHS plaquettes of that line)."""
+    import numpy as np
+    lib, err = _ref_hlm_lib()
+    if lib is None:
+        return None, err
+    c_dp = ctypes.POINTER(ctypes.c_double)
+    pots = np.zeros(N_SITES)
+    lib.ref_hlm_potentials(ctypes.c_ulong(SEED), N_SITES, 1, pots.ctypes.data_as(c_dp))
+    dim_wfs = N_PHI * N_SITES
+    wf = np.zeros(2 * (G + 1) * dim_wfs, np.complex128)
+    et = np.zeros((G + 1) * N_PHI)
+    ct = np.zeros(G * N_PHI)
+    state = {"t1": 0}
+
+    def run_line():
+        t1 = state["t1"] % (G + 1)
+        lib.ref_hlm_solve_line(t1, LX, LY, Q, BAND, G, wf.ctypes.data_as(c_dp), et.ctypes.data_as(c_dp),
+                               pots.ctypes.data_as(c_dp), threads)
+        if t1 >= 1:
+            lib.ref_peer_cal_chern(wf.ctypes.data_as(c_dp), ct.ctypes.data_as(c_dp), N_PHI, N_SITES, G, t1,
+                                   threads)
+        state["t1"] += 1
+        return G   # k-point solves in this line
+    return run_line, None
+
+
+def cpu_baseline(min_seconds=10.0, max_lines=G + 1):
+    """The reference's own CPU path timed on this host (bounded sample of the workload)."""
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    run_line, err = _ref_line_runner(threads)
+    if run_line is None:
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": err}
+    run_line()   # line theta_1 = 0 (warm-up, not timed: it has no plaquettes)
+    solves, t0 = 0, time.perf_counter()
+    lines = 0
+    while lines < max_lines - 1 and (time.perf_counter() - t0 < min_seconds or lines < 1):
+        solves += run_line()
+        lines += 1
+    dt = time.perf_counter() - t0
+    return {"value": solves / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"sample 0, theta_1 lines 1..{lines} ({solves} k-point solves: projection, "
+                      f"zheevd, back-transform, FHS) with {threads} threads, {dt:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    run_line, err = _ref_line_runner(threads)
+    if run_line is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    for _ in range(args.warmup):
+        run_line()
+    solves, times = 0, []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        solves += run_line()
+        times.append(time.perf_counter() - t)
+    total = sum(times)
+    value = solves / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": _config({"reference_step": f"one theta_1 line ({G} k-point solves + FHS) of sample 0"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} theta_1 lines of sample 0, {threads} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------- GPU arm
+def _traffic_per_matrix(kernel):
+    """DRAM bytes per matrix of `kernel` from the committed ncu capture summary, if any."""
+    path = os.path.join(REPO, "profiles", "dram_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+# algorithmic FP64 flops per matrix of n_phi (LAPACK counts: zhetrd 16/3 n^3, zunmtr 8 n^3)
+def _kernel_flops_per_matrix(kernel, n):
+    return {"k_hetrd": 16.0 / 3.0 * n ** 3, "k_ormtr": 8.0 * n ** 3}.get(kernel)
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import rlmb
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    ctx = rlmb.Context(local)
+    pots_h = rlmb.hlm_potentials(SEED + rank, N_SITES, NS)
+    d_pot = torch.tensor(pots_h, device="cuda")
+    d_e = torch.empty((NS, N_PHI), dtype=torch.float64, device="cuda")
+    d_c = torch.empty((NS, N_PHI), dtype=torch.float64, device="cuda")
+    pinned = torch.from_numpy(pots_h).pin_memory()
+
+    def step_device():
+        ctx.hlm_mesh_solve_device(LX, LY, Q, BAND, G, d_pot, d_e, d_c)
+
+    def step_e2e():
+        return ctx.hlm_mesh_solve(LX, LY, Q, BAND, G, pinned.numpy())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step_device()
+    barrier()
+    # ---- value: device-resident inputs
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ctx.profile(True)
+    launches0 = ctx.launches
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step_device()
+    ev1.record()
+    barrier()
+    ms_dev = max_over_ranks(ev0.elapsed_time(ev1))
+    launches = ctx.launches - launches0
+    prof = ctx.profile_report()
+    ctx.profile(False)
+    clk = clocks.stop()
+    # results sanity (sum rule and integrality of the Chern numbers of every sample)
+    c = d_c.cpu().numpy()
+    chern_ok = bool(np.abs(c - np.rint(c)).max() < 1e-6 and np.abs(c.sum(axis=1) - 1).max() < 1e-6)
+    # ---- e2e: host buffers through the C ABI
+    step_e2e()
+    barrier()
+    ev0.record()
+    for _ in range(args.steps):
+        step_e2e()
+    ev1.record()
+    barrier()
+    ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))
+
+    value = ws * SOLVES_PER_STEP * args.steps / (ms_dev * 1e-3)
+    e2e = ws * SOLVES_PER_STEP * args.steps / (ms_e2e * 1e-3)
+    line = None
+    if rank == 0:
+        peak = ctx.fp64_peak_tflops()
+        # dominant kernel of the timed region and its roofline
+        top = max(prof.items(), key=lambda kv: kv[1][0])
+        kname, (kms, klaunch) = top
+        fpm = _kernel_flops_per_matrix(kname, N_PHI)
+        total_ms = sum(v[0] for v in prof.values())
+        roof = None
+        if fpm is not None:
+            matrices_per_launch = SOLVES_PER_STEP * args.steps / klaunch
+            achieved = fpm * matrices_per_launch / (kms / klaunch * 1e-3) / 1e12
+            tr = _traffic_per_matrix(kname)
+            roof = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak,
+                    "traffic": tr * matrices_per_launch if tr is not None else None,
+                    "peak_source": "measured in this run: FP64 FMA throughput probe "
+                                   "(MEASURED_PEAKS.json holds no FP64 figure)",
+                    "share_of_gpu_time": kms / total_ms}
+        eig_ms = sum(prof.get(k, (0, 0))[0] for k in ("k_hetrd", "k_tridiag", "k_ormtr"))
+        eig_tflops = 13.33 * N_PHI ** 3 * SOLVES_PER_STEP * args.steps / (eig_ms * 1e-3) / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config({"parallelism": f"replicas x{ws} (sample-sharded)",
+                               "samples_per_hour": value / KPTS * 3600.0,
+                               "chern_integral_and_sum_rule_ok": chern_ok}),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(pots_h.nbytes),
+                    "d2h_bytes_per_step": int(2 * NS * N_PHI * 8)},
+            "roofline": roof,
+            "eigensolve_roofline": {"flops_per_solve": "13.33 n^3", "achieved_tflops": eig_tflops,
+                                    "peak_tflops": peak, "frac": eig_tflops / peak},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+    if ws > 1:
+        dist.barrier()
+    ctx.close()
+    if rank == 0:
+        line["cpu_baseline"] = cpu_baseline() if ws == 1 else None
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,130 @@
+/*
+ * rlm_b200.h -- C ABI of the B200 (sm_100a) twist-mesh pipeline for the random
+ * Landau-level model (rlm) and the Hofstadter lattice model (hlm).
+ *
+ * Conventions (those of the reference, qiongz/Random-Landau-Model):
+ *   - complex numbers are interleaved double pairs (re, im), i.e. the memory layout of
+ *     std::complex<double>; a "complex array of length L" is 2*L doubles;
+ *   - matrices are column-major with leading dimension n; Hermitian input is read from
+ *     the upper triangle (LAPACK uplo='U'), as diag_wrappers/mkl_diag.cpp:2-9 does;
+ *   - eigenvalues ascend; eigenvector k overwrites column k (elements [k*n, k*n+n));
+ *   - arguments named d_* are device pointers, h_* host pointers;
+ *   - every call returns an int status: 0 success, <0 argument/CUDA/allocation error,
+ *     >0 number of matrices whose eigensolve did not converge.
+ * All device work is queued on the context's stream; functions returning host results
+ * synchronise that stream.  A context is bound to one device and is not thread-safe;
+ * use one context per host thread.
+ */
+#ifndef RLM_B200_H
+#define RLM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RLMB_OK 0
+#define RLMB_ERR_ARG -1
+#define RLMB_ERR_CUDA -2
+#define RLMB_ERR_ALLOC -3
+#define RLMB_ERR_NO_DEVICE -4
+
+typedef struct rlmb_context rlmb_context;
+
+/* ------------------------------------------------------------------ context */
+int rlmb_create(rlmb_context** ctx, int device);
+int rlmb_destroy(rlmb_context* ctx);
+/* stream: a cudaStream_t (0 = the legacy default stream). */
+int rlmb_set_stream(rlmb_context* ctx, void* stream);
+const char* rlmb_status_string(int status);
+/* Number of kernel launches this context has issued since creation. */
+long long rlmb_launch_count(const rlmb_context* ctx);
+/* Per-kernel timing with CUDA events recorded on the context stream around every launch
+ * (no counterpart in the reference, whose drivers time whole phases with cudaEvent /
+ * std::chrono, rlm/main_rlm_gpu.cu:115-283).  enable clears the accumulators;
+ * count synchronises the stream and returns the number of kernels seen; entry i gives
+ * the kernel name, its summed device time and its number of launches. */
+int rlmb_profile_enable(rlmb_context* ctx, int on);
+int rlmb_profile_count(rlmb_context* ctx);
+int rlmb_profile_entry(rlmb_context* ctx, int index, char* name, int name_cap, double* total_ms,
+                       long long* launches);
+/* Measured double-precision FMA throughput of the device (TFLOP/s), the roofline
+ * denominator of the FP64 kernels. */
+int rlmb_probe_fp64_peak(rlmb_context* ctx, double* tflops);
+
+/* ------------------------------------------------- (b) Hermitian eigensolver
+ * Batched full eigendecomposition, double precision, in place.
+ * Replaces: mkl_heevd            diag_wrappers/mkl_diag.cpp:2-9   (host, col-major, 'U')
+ *           cusolver_diag_hamil  diag_wrappers/cusolver_diag.cu:3-22
+ *           magma_diag_hamil     diag_wrappers/magma_diag.cu:2-49
+ * d_a:    batch matrices of n*n complex, col-major, upper triangle read; on return
+ *         column k of matrix b holds eigenvector k.
+ * d_w:    batch*n eigenvalues, ascending per matrix.
+ * d_info: optional (may be NULL) batch ints: 0 ok, >0 eigenvectors not converged. */
+int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch, int* d_info);
+/* Host-pointer form of the same call (copies in and out): the drop-in for mkl_heevd. */
+int rlmb_heevd_host(rlmb_context* ctx, double* h_a, double* h_w, int n, int batch);
+
+/* ------------------------------------------------------- (a) rlm assembly
+ * Disorder-independent coefficient tables, computed on the host exactly as
+ * rlm/matrix_coefficients.cpp:3-25 (prepare_coeff) does, bit for bit:
+ * coeff_mn[dim*dim], coeff_m_theta[(n_mesh+1)*dim], coeff_jm[n_phi*dim] (complex). */
+int rlmb_rlm_coeff_tables(int n_phi, int off_head, int dim, int n_mesh, double L1, double L2,
+                          double* h_coeff_mn, double* h_coeff_m_theta, double* h_coeff_jm);
+/* Impurities of one sample, as rlm/disorder_potential.cpp:3-21 draws them (host MT19937). */
+int rlmb_rlm_disorder(int impurity_num, double L1, double L2, unsigned long seed, int sample,
+                      double* h_x, double* h_y, double* h_s);
+/* V_mn of one or more samples (rlm/matrix_coefficients.cpp:27-44, rlm/potential_coeff.cu:3-26):
+ * d_x,d_y,d_s: n_samples*impurity_num; d_vmn: n_samples*dim*dim complex, row-major m*dim+n. */
+int rlmb_rlm_potential(rlmb_context* ctx, const double* d_x, const double* d_y, const double* d_s,
+                       int impurity_num, int n_samples, const double* d_coeff_mn, int dim,
+                       int off_head, double* d_vmn);
+/* H(theta_1, theta_2) for `count` k-points of one sample (rlm/hamiltonian_rlm_cpu.cpp:14-48,
+ * rlm/hamiltonian_rlm_gpu.cu:9-50): d_h receives count matrices of n_phi*n_phi complex,
+ * filled as the reference fills its buffer (row-major H, lower = conj(upper)), which is the
+ * column-major upper triangle the eigensolver reads.  h_theta1/h_theta2: host int[count]. */
+int rlmb_rlm_assemble(rlmb_context* ctx, const double* d_vmn, const double* d_coeff_m_theta,
+                      const double* d_coeff_jm, int n_phi, int dim, int off_head, int n_mesh,
+                      const int* h_theta1, const int* h_theta2, int count, double* d_h);
+
+/* ------------------------------------------------------- (a) hlm assembly
+ * On-site potentials of n_sample samples from one run-long stream
+ * (hlm/main_hlm_cpu.cpp:345-358): h_out[n_sample*n_sites]. */
+int rlmb_hlm_potentials(unsigned long seed, int n_sites, int n_sample, double* h_out);
+/* Clean Bloch basis W(theta_1,theta_2) of band `band` (hlm/hamiltonian_hlm_cpu.cpp:2-56):
+ * d_wfs receives n_sites*n_phi complex, column-major (column kx*ly+ky). */
+int rlmb_hlm_basis(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh, int theta_1,
+                   int theta_2, double* d_wfs);
+/* Projected H = W^H diag(V) W for `count` k-points of one sample
+ * (hlm/hamiltonian_hlm_cpu.cpp:173-176): d_h receives count column-major n_phi*n_phi. */
+int rlmb_hlm_project(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh,
+                     const double* d_potential, const int* h_theta1, const int* h_theta2,
+                     int count, double* d_h);
+
+/* --------------------------------------------------------- (c) FHS Chern step
+ * Plaquette phases between two adjacent theta_1 lines (diag_wrappers/chern.cpp:3-75):
+ * d_prev, d_cur: (n_mesh+1) k-points of n_phi states each, state k of k-point t at
+ * [(t*n_phi + k)*dim_vec]; d_chern_theta: n_mesh*n_phi, entry [m + k*n_mesh] =
+ * -arg(prod)/2pi exactly as the reference stores it. */
+int rlmb_fhs_line(rlmb_context* ctx, const double* d_prev, const double* d_cur, int n_phi,
+                  int dim_vec, int n_mesh, double* d_chern_theta);
+
+/* ------------------------------------------------------- whole-mesh pipelines
+ * rlm: samples sample0 .. sample0+n_samples-1 of the rlm_cpu_dp run with these options
+ * (rlm/main_rlm_cpu.cpp:109-243); h_energies/h_chern: n_samples*n_phi, the two columns
+ * the reference writes to energy_Chern_No.txt (twist-averaged energy, Chern number). */
+int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double quanta_concentration,
+                        double impurity_concentration, int n_mesh, unsigned long seed,
+                        int sample0, int n_samples, double* h_energies, double* h_chern);
+/* hlm: n_samples samples with the given potentials (hlm/main_hlm_cpu.cpp:354-475). */
+int rlmb_hlm_mesh_solve(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh,
+                        const double* h_potentials, int n_samples, double* h_energies,
+                        double* h_chern);
+/* Device-resident form: potentials, energies and Chern numbers stay in device memory. */
+int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh,
+                               const double* d_potentials, int n_samples, double* d_energies,
+                               double* d_chern);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

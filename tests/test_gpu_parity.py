@@ -1,0 +1,281 @@
+"""GPU parity of every pipeline stage, called through the C ABI, against the oracle and the
+reference's golden fixtures.
+
+Tolerances (double precision throughout):
+  eigenvalues        max|w - w_ref| <= 1e-12 * max|w_ref|   (reference: zheevd)
+  residual           ||M X - X diag(w)||_F <= 1e-12 * ||M||_F
+  orthogonality      ||X^H X - I||_F <= 1e-11
+  H / V_mn entries   max|H - H_ref| <= 1e-12 * max|H_ref|
+  Chern numbers      rint() identical, |C - C_ref| <= 1e-8
+  twist energies     max|E - E_ref| <= 1e-10 * max|E_ref|
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import rlmb
+    c = rlmb.Context(0)
+    yield c
+    c.close()
+
+
+def _hermitian(rng, n, kind="random"):
+    if kind == "random":
+        a = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+        return (a + a.conj().T) / 2
+    if kind == "identity":
+        return np.eye(n, dtype=np.complex128)
+    if kind == "degenerate":
+        q = np.linalg.qr(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))[0]
+        w = np.repeat(np.arange((n + 2) // 3, dtype=float), 3)[:n]
+        return (q * w) @ q.conj().T
+    if kind == "diagonal":
+        return np.diag(rng.normal(size=n)).astype(np.complex128)
+    if kind == "zero":
+        return np.zeros((n, n), np.complex128)
+    if kind == "blocks":
+        h = np.zeros((n, n), np.complex128)
+        b = _hermitian(rng, n // 2)
+        h[: n // 2, : n // 2] = b
+        h[n // 2 : 2 * (n // 2), n // 2 : 2 * (n // 2)] = b
+        if n % 2:
+            h[-1, -1] = 0.25
+        return h
+    if kind == "tridiag_split":
+        h = np.diag(rng.normal(size=n)).astype(np.complex128)
+        for i in range(n - 1):
+            if i % 5 != 4:
+                h[i, i + 1] = rng.normal() + 1j * rng.normal()
+                h[i + 1, i] = np.conj(h[i, i + 1])
+        return h
+    raise ValueError(kind)
+
+
+def _check_eig(M, w, X, wref):
+    scale = max(np.abs(wref).max(), 1e-300)
+    assert np.abs(w - wref).max() <= 1e-12 * scale + 1e-300, np.abs(w - wref).max() / scale
+    nrm = max(np.linalg.norm(M), 1e-300)
+    res = np.linalg.norm(M @ X - X * w[None, :])
+    assert res <= 1e-12 * nrm + 1e-300, res / nrm
+    orth = np.linalg.norm(X.conj().T @ X - np.eye(M.shape[0]))
+    assert orth <= 1e-11, orth
+
+
+def _run_heevd(ctx, mats):
+    n = mats[0].shape[0]
+    a = torch.tensor(np.stack([m.T for m in mats]), dtype=torch.complex128, device="cuda").contiguous()
+    info = torch.zeros(len(mats), dtype=torch.int32, device="cuda")
+    w = ctx.heevd(a, info=info)
+    torch.cuda.synchronize()
+    assert int(info.abs().sum()) == 0
+    X = a.cpu().numpy()   # row k = eigenvector k
+    return w.cpu().numpy(), [X[b].T for b in range(len(mats))]
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 31, 32, 33, 64, 100, 128, 256])
+def test_heevd_random(ctx, n):
+    rng = np.random.default_rng(n)
+    mats = [_hermitian(rng, n) for _ in range(3)]
+    w, X = _run_heevd(ctx, mats)
+    for b, M in enumerate(mats):
+        _check_eig(M, w[b], X[b], np.linalg.eigvalsh(M))
+
+
+@pytest.mark.parametrize("kind", ["identity", "degenerate", "diagonal", "zero", "blocks", "tridiag_split"])
+@pytest.mark.parametrize("n", [7, 48])
+def test_heevd_structured(ctx, kind, n):
+    rng = np.random.default_rng(7 * n)
+    M = _hermitian(rng, n, kind)
+    w, X = _run_heevd(ctx, [M])
+    wref = np.linalg.eigvalsh(M)
+    if kind == "zero":
+        assert np.abs(w[0]).max() == 0.0
+        assert np.linalg.norm(X[0].conj().T @ X[0] - np.eye(n)) <= 1e-11
+        return
+    _check_eig(M, w[0], X[0], wref)
+
+
+def test_heevd_reads_upper_triangle_only(ctx):
+    rng = np.random.default_rng(3)
+    M = _hermitian(rng, 20)
+    buf = M.copy()
+    buf[np.tril_indices(20, -1)] = 1e3 + 7j   # garbage below the diagonal, as LAPACK 'U' allows
+    buf[np.diag_indices(20)] += 0.5j          # imaginary diagonal parts are ignored
+    w, X = _run_heevd(ctx, [buf])
+    _check_eig(M, w[0], X[0], np.linalg.eigvalsh(M))
+
+
+def test_mkl_heevd_host_dropin(ctx):
+    rng = np.random.default_rng(11)
+    M = _hermitian(rng, 24)
+    w, vec = ctx.mkl_heevd(M.T.reshape(-1).copy(), 24)   # column-major buffer
+    X = vec.reshape(24, 24).T
+    _check_eig(M, w, X, np.linalg.eigvalsh(M))
+
+
+# -------------------------------------------------------------------------- rlm stages
+def _rlm_setup(d):
+    import rlmb
+    n_phi, g = int(d["n_phi"]), int(d["n_mesh"])
+    p = rlmb.rlm_params(n_phi, float(d["qc"]), float(d["ic"]))
+    return n_phi, g, p
+
+
+@pytest.mark.parametrize("name", ["rlm_n16_g8_c2_s1.npz", "rlm_n64_g4_c1_s3.npz", "rlm_n128_g2_c1_s5.npz"])
+def test_rlm_potential_matches_reference(ctx, name):
+    d = golden(name)
+    n_phi, g, p = _rlm_setup(d)
+    ns = int(d["n_sample"])
+    x = torch.tensor(d["x"], device="cuda")
+    y = torch.tensor(d["y"], device="cuda")
+    s = torch.tensor(d["s"], device="cuda")
+    cmn = torch.tensor(d["coeff_mn"], device="cuda")
+    v = ctx.rlm_potential(x, y, s, cmn, p["off_head"]).cpu().numpy()
+    for n in range(ns):
+        ref = d["v_mn"][n]
+        assert np.abs(v[n] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["rlm_n16_g8_c2_s1.npz", "rlm_n32_g4_c1_s7.npz", "rlm_n128_g2_c1_s5.npz"])
+def test_rlm_assemble_matches_oracle(ctx, name):
+    from oracle import rlm as orlm
+    d = golden(name)
+    n_phi, g, p = _rlm_setup(d)
+    op = orlm.RlmParams(n_phi, float(d["qc"]), float(d["ic"]), g, 1, int(d["seed"]))
+    vmn = d["v_mn"][0]
+    t1 = np.array([0, 1, g, g // 2, 0], np.int32)
+    t2 = np.array([0, g, 1, g // 2, g], np.int32)
+    H = ctx.rlm_assemble(torch.tensor(vmn, device="cuda"), torch.tensor(d["coeff_m_theta"], device="cuda"),
+                         torch.tensor(d["coeff_jm"], device="cuda"), n_phi, p["off_head"], g, t1, t2)
+    H = H.cpu().numpy()
+    for i in range(len(t1)):
+        ref = orlm.assemble(op, vmn, d["coeff_m_theta"], d["coeff_jm"], int(t1[i]), int(t2[i]))
+        ref = ref.reshape(n_phi, n_phi)
+        assert np.abs(H[i] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_rlm_eigenpairs_match_reference_kpoints(ctx):
+    """Assemble + eigensolve at k-points whose reference eigenvectors are recorded."""
+    from oracle import rlm as orlm
+    for name in ("rlm_n16_g8_c2_s1.npz", "rlm_n32_g4_c1_s7.npz", "rlm_n64_g4_c1_s3.npz"):
+        d = golden(name)
+        n_phi, g, p = _rlm_setup(d)
+        for key in d.files:
+            if not key.startswith("eigvec_s"):
+                continue
+            _, sn, k1, k2 = key.split("_")
+            sample, k1, k2 = int(sn[1:]), int(k1), int(k2)
+            H = ctx.rlm_assemble(torch.tensor(d["v_mn"][sample], device="cuda"),
+                                 torch.tensor(d["coeff_m_theta"], device="cuda"),
+                                 torch.tensor(d["coeff_jm"], device="cuda"), n_phi, p["off_head"], g,
+                                 [k1], [k2])
+            w = ctx.heevd(H)
+            torch.cuda.synchronize()
+            wref = d["energies_mesh"][sample][k1, k2]
+            assert np.abs(w.cpu().numpy()[0] - wref).max() <= 1e-12 * np.abs(wref).max()
+            Xr = d[key].reshape(n_phi, n_phi)   # row n = reference eigenvector n
+            Xg = H.cpu().numpy()[0]
+            ov = np.abs(np.einsum("nr,nr->n", np.conj(Xr), Xg))
+            assert np.abs(ov - 1).max() < 1e-9
+
+
+@pytest.mark.parametrize("name", ["rlm_n16_g8_c2_s1.npz", "rlm_n32_g4_c1_s7.npz"])
+def test_fhs_line_matches_oracle(ctx, name):
+    from oracle import fhs, rlm as orlm
+    d = golden(name)
+    n_phi, g, p = _rlm_setup(d)
+    op = orlm.RlmParams(n_phi, float(d["qc"]), float(d["ic"]), g, 1, int(d["seed"]))
+    r = orlm.run_sample(op, 0, keep=True)
+    X = r["eigvecs"]
+    for t1 in (1, g):
+        ref = fhs.line_chern(X[t1 - 1], X[t1])          # [g, N]
+        out = ctx.fhs_line(torch.tensor(X[t1 - 1], device="cuda"), torch.tensor(X[t1], device="cuda"))
+        assert np.abs(out.cpu().numpy().T - ref).max() < 1e-10
+
+
+RLM_MESH = ["rlm_n16_g8_c2_s1.npz", "rlm_n32_g4_c1_s7.npz", "rlm_n64_g4_c1_s3.npz",
+            "rlm_n128_g2_c1_s5.npz", "rlm_n16_g64_c2_s1.npz"]
+
+
+@pytest.mark.parametrize("name", RLM_MESH)
+def test_rlm_mesh_solve_matches_reference(ctx, name):
+    d = golden(name)
+    n_phi, g, p = _rlm_setup(d)
+    ns = int(d["n_sample"])
+    e, c = ctx.rlm_mesh_solve(n_phi, float(d["qc"]), float(d["ic"]), g, int(d["seed"]), 0, ns)
+    for n in range(ns):
+        eref, cref = d["energies"][n], d["chern"][n]
+        assert np.abs(e[n] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[n]), np.rint(cref))
+        assert np.abs(c[n] - cref).max() < 1e-8
+
+
+def test_rlm_mesh_solve_sample_offset(ctx):
+    d = golden("rlm_n16_g8_c2_s1.npz")
+    e, c = ctx.rlm_mesh_solve(16, 1.0, 16.0, 8, 1, 1, 1)
+    assert np.abs(e[0] - d["energies"][1]).max() <= 1e-10 * np.abs(d["energies"][1]).max()
+    assert np.array_equal(np.rint(c[0]), np.rint(d["chern"][1]))
+
+
+# -------------------------------------------------------------------------- hlm stages
+@pytest.mark.parametrize("name", ["hlm_6x6_q3_b0_g8_c2_s1.npz", "hlm_9x6_q3_b1_g8_c1_s2.npz",
+                                  "hlm_8x8_q2_b0_g4_c1_s4.npz"])
+def test_hlm_basis_matches_reference(ctx, name):
+    d = golden(name)
+    lx, ly, Q, b, g = (int(d[k]) for k in ("lx", "ly", "Q", "band", "n_mesh"))
+    for key in d.files:
+        if not key.startswith("basis_"):
+            continue
+        _, t1, t2 = key.split("_")
+        W = ctx.hlm_basis(lx, ly, Q, b, g, int(t1), int(t2)).cpu().numpy()
+        Wr = d[key].reshape(-1, lx * ly)
+        ov = np.abs(np.einsum("cr,cr->c", np.conj(Wr), W))
+        assert np.abs(ov - 1).max() < 1e-12
+
+
+@pytest.mark.parametrize("name", ["hlm_6x6_q3_b0_g8_c2_s1.npz", "hlm_12x8_q3_b2_g8_c1_s2.npz",
+                                  "hlm_48x16_q3_b0_g2_c1_s1.npz"])
+def test_hlm_project_spectrum_matches_reference(ctx, name):
+    d = golden(name)
+    lx, ly, Q, b, g = (int(d[k]) for k in ("lx", "ly", "Q", "band", "n_mesh"))
+    pot = torch.tensor(d["potentials"][0], device="cuda")
+    t1 = np.array([0, 1, g, g], np.int32)
+    t2 = np.array([0, g - 1, 0, g // 2], np.int32)
+    H = ctx.hlm_project(lx, ly, Q, b, g, pot, t1, t2)
+    Hn = H.cpu().numpy()
+    for i in range(len(t1)):
+        M = Hn[i].T
+        assert np.abs(M - M.conj().T).max() < 1e-14 * max(1.0, np.abs(M).max())
+        wref = d["energies_mesh"][0][t1[i], t2[i]]
+        w = np.linalg.eigvalsh(M)
+        assert np.abs(w - wref).max() <= 1e-12 * np.abs(wref).max()
+    w = ctx.heevd(H).cpu().numpy()
+    for i in range(len(t1)):
+        wref = d["energies_mesh"][0][t1[i], t2[i]]
+        assert np.abs(w[i] - wref).max() <= 1e-12 * np.abs(wref).max()
+
+
+HLM_MESH = ["hlm_3x3_q3_g64_c2_s1.npz", "hlm_6x6_q3_b0_g8_c2_s1.npz", "hlm_9x6_q3_b1_g8_c1_s2.npz",
+            "hlm_12x8_q3_b2_g8_c1_s2.npz", "hlm_48x16_q3_b0_g2_c1_s1.npz"]
+
+
+@pytest.mark.parametrize("name", HLM_MESH)
+def test_hlm_mesh_solve_matches_reference(ctx, name):
+    d = golden(name)
+    lx, ly, Q, b, g = (int(d[k]) for k in ("lx", "ly", "Q", "band", "n_mesh"))
+    e, c = ctx.hlm_mesh_solve(lx, ly, Q, b, g, d["potentials"])
+    for n in range(int(d["n_sample"])):
+        eref, cref = d["energies"][n], d["chern"][n]
+        assert np.abs(e[n] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[n]), np.rint(cref))
+        assert np.abs(c[n] - cref).max() < 1e-8
