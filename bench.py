@@ -271,9 +271,11 @@ def run_gpu(args):
     prof = ctx.profile_report()
     ctx.profile(False)
     clk = clocks.stop()
-    # results sanity (sum rule and integrality of the Chern numbers of every sample)
+    # results sanity: every Chern number integral (the per-state FHS sum need not be 1: the
+    # reference gives 2 or 0 for some samples of this mesh as well, e.g. seed 1 samples 5, 22)
     c = d_c.cpu().numpy()
-    chern_ok = bool(np.abs(c - np.rint(c)).max() < 1e-6 and np.abs(c.sum(axis=1) - 1).max() < 1e-6)
+    chern_ok = bool(np.abs(c - np.rint(c)).max() < 1e-6)
+    sum_rule_fraction = float(np.mean(np.abs(c.sum(axis=1) - 1) < 1e-6))
     # ---- e2e: host buffers through the C ABI
     step_e2e()
     barrier()
@@ -313,7 +315,9 @@ def run_gpu(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": _config({"parallelism": f"replicas x{ws} (sample-sharded)",
                                "samples_per_hour": value / KPTS * 3600.0,
-                               "chern_integral_and_sum_rule_ok": chern_ok}),
+                               "chern_integral": chern_ok,
+                               "fraction_of_samples_with_sum_1": sum_rule_fraction,
+                               "eigensolve_failures": int(ctx.last_failures)}),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(pots_h.nbytes),
                     "d2h_bytes_per_step": int(2 * NS * N_PHI * 8)},
             "roofline": roof,

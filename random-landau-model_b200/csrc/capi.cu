@@ -96,6 +96,15 @@ static int hlm_tables(rlmb_context* ctx, int lx, int ly, int Q, int band, int g,
     return RLMB_OK;
 }
 
+// Adds the number of nonzero entries of d_info[0..count) to *failures (synchronous).
+static int count_failures(rlmb_context* ctx, const int* d_info, int count, long long* failures) {
+    std::vector<int> h(count);
+    RLMB_CUDA_TRY(cudaMemcpyAsync(h.data(), d_info, count * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < count; ++i) *failures += h[i] != 0;
+    return RLMB_OK;
+}
+
 static bool hlm_args_ok(int lx, int ly, int Q, int band, int g) {
     return lx > 0 && ly > 0 && Q > 0 && Q <= RLMB_MAX_Q && lx % Q == 0 && band >= 0 && band < Q &&
            g > 0 && lx / Q <= 64 && ly <= 64;
@@ -318,6 +327,7 @@ int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int 
     need<double>(bytes, (size_t)n_phi * kpts * nb);
     need<cplx>(bytes, 2 * (size_t)n_phi * kpts * nb);
     need<double>(bytes, 2 * (size_t)n_phi * nb);
+    need<int>(bytes, (size_t)kpts * nb);
     if (int rc = ensure_pipe(ctx, bytes)) return rc;
     Carver cv(ctx->pipe);
     cplx* d_cmn = cv.take<cplx>(cmn.size() / 2);
@@ -330,6 +340,8 @@ int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int 
     double* d_W = cv.take<double>((size_t)n_phi * kpts * nb);
     cplx* d_U = cv.take<cplx>(2 * (size_t)n_phi * kpts * nb);
     double* d_out = cv.take<double>(2 * (size_t)n_phi * nb);
+    int* d_info = cv.take<int>((size_t)kpts * nb);
+    long long failures = 0;
     if (int rc = ensure_pinned(ctx, std::max(3 * (size_t)nimp * nb * sizeof(double), 2 * (size_t)kpts * nb * sizeof(int))))
         return rc;
     RLMB_CUDA_TRY(cudaMemcpyAsync(d_cmn, cmn.data(), cmn.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -365,8 +377,9 @@ int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int 
         if (int rc = launch_rlm_assemble(ctx, d_vmn, d_cmt, d_cjm, d_t, d_t + (size_t)nb * kpts, cnt * kpts, kpts,
                                          n_phi, dim, o, d_H))
             return rc;
-        const int bad = rlmb_heevd_batched(ctx, reinterpret_cast<double*>(d_H), d_W, n_phi, cnt * kpts, nullptr);
-        if (bad < 0) return bad;
+        if (int rc = rlmb_heevd_batched(ctx, reinterpret_cast<double*>(d_H), d_W, n_phi, cnt * kpts, d_info))
+            return rc;
+        if (int rc = count_failures(ctx, d_info, cnt * kpts, &failures)) return rc;
         cplx* d_U1 = d_U;
         cplx* d_U2 = d_U + (size_t)n_phi * kpts * nb;
         if (int rc = launch_rlm_links(ctx, d_H, n_phi, g, cnt, d_U1, d_U2)) return rc;
@@ -378,7 +391,7 @@ int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int 
                                       (size_t)cnt * n_phi * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     }
-    return RLMB_OK;
+    return failures > 0 ? (int)std::min<long long>(failures, 1 << 30) : RLMB_OK;
 }
 
 // --------------------------------------------------------------------- hlm pipeline
@@ -404,6 +417,7 @@ int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int ban
     need<cplx>(bytes, nn * kpts * nb);
     need<double>(bytes, (size_t)N * kpts * nb);
     need<cplx>(bytes, 2 * (size_t)N * kpts * nb);
+    need<int>(bytes, (size_t)kpts * nb);
     if (int rc = ensure_pipe(ctx, bytes)) return rc;
     Carver cv(ctx->pipe);
     int* d_t = cv.take<int>(kpts);
@@ -412,6 +426,8 @@ int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int ban
     double* d_W = cv.take<double>((size_t)N * kpts * nb);
     cplx* d_U1 = cv.take<cplx>((size_t)N * kpts * nb);
     cplx* d_U2 = cv.take<cplx>((size_t)N * kpts * nb);
+    int* d_info = cv.take<int>((size_t)kpts * nb);
+    long long failures = 0;
     {
         std::vector<int> tl(kpts);
         for (int t1 = 0; t1 <= g; ++t1)
@@ -423,14 +439,15 @@ int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int ban
         const int cnt = std::min(nb, n_samples - s0);
         if (int rc = launch_hlm_vtilde(ctx, d_potentials + (size_t)s0 * ns, lx, ly, Q, cnt, d_vt)) return rc;
         if (int rc = launch_hlm_project(ctx, hb, d_vt, d_t, lx, ly, Q, kpts, cnt, d_H)) return rc;
-        const int bad = rlmb_heevd_batched(ctx, reinterpret_cast<double*>(d_H), d_W, N, cnt * kpts, nullptr);
-        if (bad < 0) return bad;
+        if (int rc = rlmb_heevd_batched(ctx, reinterpret_cast<double*>(d_H), d_W, N, cnt * kpts, d_info))
+            return rc;
+        if (int rc = count_failures(ctx, d_info, cnt * kpts, &failures)) return rc;
         if (int rc = launch_hlm_links(ctx, hb, d_H, lx, ly, Q, g, cnt, d_U1, d_U2)) return rc;
         if (int rc = launch_plaquettes(ctx, d_U1, d_U2, d_W, N, g, cnt, 1, d_energies + (size_t)s0 * N,
                                        d_chern + (size_t)s0 * N))
             return rc;
     }
-    return RLMB_OK;
+    return failures > 0 ? (int)std::min<long long>(failures, 1 << 30) : RLMB_OK;
 }
 
 int rlmb_hlm_mesh_solve(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh,

@@ -74,6 +74,25 @@ __device__ __forceinline__ cplx transpose_reduce32(cplx (&v)[32]) {
     return v[0];
 }
 
+// As transpose_reduce32 for a 16-column group: lane l (and l^16) receives the sum over
+// all 32 lanes of v[l & 15].
+__device__ __forceinline__ cplx transpose_reduce16(cplx (&v)[16]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = cadd(v[j], shfl_xor(v[j], 16));
+#pragma unroll
+    for (int s = 8; s >= 1; s >>= 1) {
+        const bool up = (lane & s) != 0;
+#pragma unroll
+        for (int j = 0; j < s; ++j) {
+            cplx send = up ? v[j] : v[j + s];
+            cplx keep = up ? v[j + s] : v[j];
+            v[j] = cadd(keep, shfl_xor(send, s));
+        }
+    }
+    return v[0];
+}
+
 __device__ __forceinline__ void tile_of(int t, int& R, int& C) {
     // t-th tile (row block R <= column block C) in column-major order of the upper triangle
     int c = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
@@ -89,128 +108,248 @@ __device__ __forceinline__ void smem_atomic_add(cplx* p, cplx v) {
 }
 
 // ------------------------------------------------------------------ k_hetrd
-// a: n*n col-major, upper triangle.  On exit: column c (c >= 1) rows 0..c-2 hold the
-// reflector of step c-1 (v[c-1] = 1 implicit), diag/offdiag in dd/ee, tau in tt.
-__global__ void __launch_bounds__(HETRD_THREADS)
-k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
-        cplx* __restrict__ TAU, int n) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* v = reinterpret_cast<cplx*>(smem_raw);   // [n] reflector
-    cplx* p = v + n;                                // [n] A v, then w
-    double* red = reinterpret_cast<double*>(p + n); // [2*warps]
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
+// Storage of the active leading block: global column-major (ld = n) while it is large,
+// packed upper triangle in shared memory (column c at c(c+1)/2) once it fits.
+struct GlobalStore {
+    cplx* a;
+    int n;
+    __device__ __forceinline__ cplx* at(int r, int c) const { return a + (size_t)c * n + r; }
+};
+struct SharedStore {
+    cplx* s;
+    __device__ __forceinline__ cplx* at(int r, int c) const { return s + (c * (c + 1) / 2 + r); }
+};
+
+// One pass over the upper triangle of the leading m x m block, 32x32 tiles dealt to
+// warps: applies the rank-2 update A -= v w^H + w v^H of the previous reflector (if upd)
+// and accumulates pn += A' vn for the next one (if acc), reading and writing every
+// stored element once.  All 32 loads of a tile are issued before any of its stores.
+template <class S>
+__device__ __forceinline__ void fused_pass(S st, int m, const cplx* __restrict__ v,
+                                           const cplx* __restrict__ w, bool upd,
+                                           const cplx* __restrict__ vn, bool acc, cplx* pn) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = HETRD_THREADS / 32;
+    const int nb = (m + 31) / 32;
+    const int ntiles = nb * (nb + 1) / 2;
+    for (int t = warp; t < ntiles; t += NW) {
+        int R, C;
+        tile_of(t, R, C);
+        const int r = R * 32 + lane;
+        const bool rin = r < m;
+        const cplx vr = rin ? v[r] : mk(0, 0);
+        const cplx wr = rin ? w[r] : mk(0, 0);
+        const cplx vnr = rin ? vn[r] : mk(0, 0);
+        cplx rowacc = mk(0, 0);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c0 = C * 32 + 16 * h;
+            if (c0 >= m) break;
+            cplx e[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int cc = c0 + j;
+                e[j] = (rin && cc < m && r <= cc) ? *st.at(r, cc) : mk(0, 0);
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int cc = c0 + j;
+                const bool valid = rin && cc < m && r <= cc;
+                cplx x = e[j];
+                if (upd) {
+                    const cplx vc = cc < m ? v[cc] : mk(0, 0);
+                    const cplx wc = cc < m ? w[cc] : mk(0, 0);
+                    cplx u = cmul(vr, cconj(wc));
+                    cfma(u, wr, cconj(vc));
+                    x = csub(x, u);
+                    if (r == cc) x.y = 0.0;
+                    if (valid) *st.at(r, cc) = x;
+                }
+                if (acc) {
+                    const cplx vnc = cc < m ? vn[cc] : mk(0, 0);
+                    if (!valid) {
+                        e[j] = mk(0, 0);
+                    } else if (r == cc) {
+                        rowacc = cadd(rowacc, cscale(vnc, x.x));
+                        e[j] = mk(0, 0);
+                    } else {
+                        cfma(rowacc, x, vnc);
+                        e[j] = cmulc(x, vnr);   // column partial: conj(A'[r][cc]) vn[r]
+                    }
+                }
+            }
+            if (acc) {
+                const cplx cs = transpose_reduce16(e);
+                const int cl = c0 + (lane & 15);
+                if (lane < 16 && cl < m) smem_atomic_add(&pn[cl], cs);
+            }
+        }
+        if (acc && rin) smem_atomic_add(&pn[r], rowacc);
+    }
+}
+
+// Householder reflector of zlarfg for (alpha, x[0..len-1]) held in col[0..len]
+// (alpha = col[len]); returns beta, tau and the scale applied to x.
+__device__ __forceinline__ void reflector(const cplx alpha, double xnorm2, double& beta, cplx& tau,
+                                          cplx& scal) {
+    if (xnorm2 == 0.0 && alpha.y == 0.0) {
+        beta = alpha.x;
+        tau = mk(0, 0);
+        scal = mk(1, 0);
+        return;
+    }
+    const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
+    beta = alpha.x >= 0.0 ? -nrm : nrm;
+    tau = mk((beta - alpha.x) / beta, -alpha.y / beta);
+    const cplx den = mk(alpha.x - beta, alpha.y);
+    const double dn = cabs2(den);
+    scal = mk(den.x / dn, -den.y / dn);
+}
+
+// Unblocked reduction A = Q T Q^H (zhetd2, uplo='U') with look-ahead: step i's rank-2
+// update and step i-1's matrix-vector product share one pass over the leading block.
+// a: n*n col-major (upper triangle).  On exit column c (c >= 1) rows 0..c-2 hold the
+// reflector of step c-1 (its entry c-1 is 1 and not stored), D/E the tridiagonal and TAU
+// the reflector scalars.  The leading block moves into shared memory once its packed
+// upper triangle fits in `tri_cap` elements.
+__global__ void __launch_bounds__(HETRD_THREADS, 2)
+k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
+        cplx* __restrict__ TAU, int n, int tri_cap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx* v = reinterpret_cast<cplx*>(smem_raw);   // [n] current reflector
+    cplx* w = v + n;                                // [n] its w vector
+    cplx* vn = w + n;                               // [n] next reflector / column buffer
+    cplx* pn = vn + n;                              // [n] A' vn accumulator
+    double* red = reinterpret_cast<double*>(pn + n);  // [2*warps]
+    cplx* tri = reinterpret_cast<cplx*>(red + 2 * (HETRD_THREADS / 32));   // packed triangle
+    const int tid = threadIdx.x;
     const size_t mat = blockIdx.x;
-    cplx* a = A + mat * (size_t)n * n;
+    GlobalStore gs{A + mat * (size_t)n * n, n};
+    SharedStore ss{tri};
     double* dd = D + mat * n;
     double* ee = E + mat * n;
     cplx* tt = TAU + mat * n;
-
-    for (int i = n - 2; i >= 0; --i) {
-        const int c = i + 1;   // column holding the vector to annihilate
-        const int m = i + 1;   // leading block rows/cols 0..i
-        // ---- (1) reflector from column c, rows 0..i  (zlarfg)
+    if (n == 1) {
+        if (tid == 0) {
+            dd[0] = gs.at(0, 0)->x;
+            ee[0] = 0.0;
+            tt[0] = mk(0, 0);
+        }
+        return;
+    }
+    bool resident = false;
+    // -- prologue: reflector of step n-2 from column n-1, then p = A v over [0..n-2]^2
+    {
+        const int i = n - 2;
         double part = 0.0;
-        for (int r = tid; r <= i; r += HETRD_THREADS) {
-            cplx x = a[(size_t)c * n + r];
-            v[r] = x;
+        for (int r = tid; r <= i + 1; r += HETRD_THREADS) {
+            const cplx x = *gs.at(r, i + 1);
+            vn[r] = x;
             if (r < i) part += cabs2(x);
         }
-        const double xnorm2 = block_sum<HETRD_THREADS>(part, red);   // syncs
-        const cplx alpha = v[i];
-        double beta = 0.0;
-        cplx tau = mk(0, 0), scal = mk(0, 0);
-        if (xnorm2 == 0.0 && alpha.y == 0.0) {
-            beta = alpha.x;
-        } else {
-            const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
-            beta = alpha.x >= 0.0 ? -nrm : nrm;
-            tau = mk((beta - alpha.x) / beta, -alpha.y / beta);
-            const cplx den = mk(alpha.x - beta, alpha.y);
-            const double dn = cabs2(den);
-            scal = mk(den.x / dn, -den.y / dn);
-        }
-        const bool active = !(tau.x == 0.0 && tau.y == 0.0);
+        const double xn2 = block_sum<HETRD_THREADS>(part, red);
+        double beta;
+        cplx tau, scal;
+        reflector(vn[i], xn2, beta, tau, scal);
+        const bool act = !(tau.x == 0.0 && tau.y == 0.0);
         __syncthreads();
         for (int r = tid; r < i; r += HETRD_THREADS) {
-            cplx x = active ? cmul(scal, v[r]) : v[r];
+            const cplx x = act ? cmul(scal, vn[r]) : vn[r];
             v[r] = x;
-            a[(size_t)c * n + r] = x;
+            *gs.at(r, i + 1) = x;
+        }
+        for (int r = tid; r < n; r += HETRD_THREADS) {
+            w[r] = mk(0, 0);
+            pn[r] = mk(0, 0);
         }
         if (tid == 0) {
             v[i] = mk(1.0, 0.0);
-            a[(size_t)c * n + i] = mk(beta, 0.0);
+            dd[n - 1] = vn[n - 1].x;
+            *gs.at(i, i + 1) = mk(beta, 0.0);
             ee[i] = beta;
             tt[i] = tau;
         }
-        for (int r = tid; r < m; r += HETRD_THREADS) p[r] = mk(0, 0);
         __syncthreads();
-        if (active) {
-            // ---- (2) p = A(0:i,0:i) v over 32x32 tiles of the upper triangle
-            const int nb = (m + 31) / 32;
-            const int ntiles = nb * (nb + 1) / 2;
-            for (int t = warp; t < ntiles; t += NW) {
-                int R, C;
-                tile_of(t, R, C);
-                const int r = R * 32 + lane;
-                const cplx vr = r < m ? v[r] : mk(0, 0);
-                cplx rowacc = mk(0, 0);
-                cplx col[32];
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int cc = C * 32 + j;
-                    cplx e = mk(0, 0);
-                    if (r < m && cc < m && r <= cc) e = a[(size_t)cc * n + r];
-                    const cplx vc = cc < m ? v[cc] : mk(0, 0);
-                    if (r == cc) {
-                        rowacc = cadd(rowacc, cscale(vc, e.x));
-                        col[j] = mk(0, 0);
-                    } else {
-                        cfma(rowacc, e, vc);
-                        col[j] = cmulc(e, vr);
-                    }
-                }
-                const cplx cs = transpose_reduce32(col);
-                if (r < m) smem_atomic_add(&p[r], rowacc);
-                const int cl = C * 32 + lane;
-                if (cl < m) smem_atomic_add(&p[cl], cs);
-            }
-            __syncthreads();
-            // ---- (3) x = tau p;  alpha2 = -tau/2 (x^H v);  w = x + alpha2 v
-            cplx dpart = mk(0, 0);
-            for (int r = tid; r < m; r += HETRD_THREADS) {
-                const cplx x = cmul(tau, p[r]);
-                p[r] = x;
-                cfmac(dpart, x, v[r]);
-            }
-            const cplx xv = block_sum<HETRD_THREADS>(dpart, red);   // syncs
-            const cplx al = cscale(cmul(tau, xv), -0.5);
-            for (int r = tid; r < m; r += HETRD_THREADS) cfma(p[r], al, v[r]);
-            __syncthreads();
-            // ---- (4) A(0:i,0:i) -= v w^H + w v^H  (upper triangle, diagonal kept real)
-            for (int cc = warp; cc < m; cc += NW) {
-                const cplx vc = v[cc], wc = p[cc];
-                for (int r = lane; r <= cc; r += 32) {
-                    cplx e = a[(size_t)cc * n + r];
-                    const cplx vr = v[r], wr = p[r];
-                    // e -= v_r conj(w_c) + w_r conj(v_c)
-                    cplx u = cmul(vr, cconj(wc));
-                    cfma(u, wr, cconj(vc));
-                    e = csub(e, u);
-                    if (r == cc) e.y = 0.0;
-                    a[(size_t)cc * n + r] = e;
-                }
-            }
-            __syncthreads();
-        } else {
-            if (tid == 0) a[(size_t)i * n + i].y = 0.0;
+        fused_pass(gs, i + 1, v, w, false, v, act, pn);
+        __syncthreads();
+        cplx dpart = mk(0, 0);
+        for (int r = tid; r <= i; r += HETRD_THREADS) {
+            const cplx x = cmul(tau, pn[r]);
+            pn[r] = x;
+            cfmac(dpart, x, v[r]);
+        }
+        const cplx xv = block_sum<HETRD_THREADS>(dpart, red);
+        const cplx al = cscale(cmul(tau, xv), -0.5);
+        for (int r = tid; r <= i; r += HETRD_THREADS) w[r] = cadd(pn[r], cmul(al, v[r]));
+        __syncthreads();
+    }
+    // -- main loop: v, w belong to step i (column i+1 done); finish column i, build the
+    //    reflector of step i-1 from it, then one fused pass over [0..i-1]^2
+    for (int i = n - 2; i >= 1; --i) {
+        if (!resident && (i + 1) * (i + 2) / 2 <= tri_cap) {
+            // move the leading (i+1)x(i+1) upper triangle into shared memory
+            for (int c = 0; c <= i; ++c)
+                for (int r = tid; r <= c; r += HETRD_THREADS) *ss.at(r, c) = *gs.at(r, c);
+            resident = true;
             __syncthreads();
         }
-        if (tid == 0) dd[c] = a[(size_t)c * n + c].x;
+        // (1) updated column i, rows 0..i
+        double part = 0.0;
+        const cplx wi = w[i], vi = v[i];
+        for (int r = tid; r <= i; r += HETRD_THREADS) {
+            cplx x = resident ? *ss.at(r, i) : *gs.at(r, i);
+            cplx u = cmul(v[r], cconj(wi));
+            cfma(u, w[r], cconj(vi));
+            x = csub(x, u);
+            vn[r] = x;
+            if (r < i - 1) part += cabs2(x);
+            pn[r] = mk(0, 0);
+        }
+        const double xn2 = block_sum<HETRD_THREADS>(part, red);
+        // (2) reflector of step i-1: alpha = A'[i-1][i], x = A'[0..i-2][i]
+        double beta;
+        cplx tau, scal;
+        reflector(vn[i - 1], xn2, beta, tau, scal);
+        const bool act = !(tau.x == 0.0 && tau.y == 0.0);
+        __syncthreads();
+        if (tid == 0) dd[i] = vn[i].x;
+        for (int r = tid; r < i - 1; r += HETRD_THREADS) {
+            const cplx x = act ? cmul(scal, vn[r]) : vn[r];
+            vn[r] = x;
+            *gs.at(r, i) = x;   // reflector storage stays in global memory
+        }
+        if (tid == 0) {
+            vn[i - 1] = mk(1.0, 0.0);
+            *gs.at(i - 1, i) = mk(beta, 0.0);
+            ee[i - 1] = beta;
+            tt[i - 1] = tau;
+        }
+        __syncthreads();
+        // (3) fused pass: update [0..i-1]^2 with (v, w), accumulate pn = A' vn
+        if (resident) fused_pass(ss, i, v, w, true, vn, act, pn);
+        else fused_pass(gs, i, v, w, true, vn, act, pn);
+        __syncthreads();
+        // (4) w' = tau pn - tau/2 (x^H vn) vn; v <- vn
+        cplx dpart = mk(0, 0);
+        for (int r = tid; r < i; r += HETRD_THREADS) {
+            const cplx x = cmul(tau, pn[r]);
+            pn[r] = x;
+            cfmac(dpart, x, vn[r]);
+        }
+        const cplx xv = block_sum<HETRD_THREADS>(dpart, red);
+        const cplx al = cscale(cmul(tau, xv), -0.5);
+        for (int r = tid; r < i; r += HETRD_THREADS) {
+            w[r] = act ? cadd(pn[r], cmul(al, vn[r])) : mk(0, 0);
+            v[r] = vn[r];
+        }
+        __syncthreads();
     }
+    // -- step 0's update reaches only A[0][0]
     if (tid == 0) {
-        dd[0] = a[0].x;
+        cplx x = resident ? *ss.at(0, 0) : *gs.at(0, 0);
+        cplx u = cmul(v[0], cconj(w[0]));
+        cfma(u, w[0], cconj(v[0]));
+        dd[0] = x.x - u.x;
         ee[n - 1] = 0.0;
         tt[n - 1] = mk(0, 0);
     }
@@ -298,6 +437,25 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
     }
     __syncthreads();
     const double pivmin = s_pivmin, onenrm = s_onenrm;
+    if (!(onenrm > 1e3 * DBL_MIN)) {
+        // T = 0 to underflow: eigenvalues are the diagonal (sorted), eigenvectors unit vectors
+        if (tid == 0) {
+            for (int k = 0; k < n; ++k) leader[k] = k;
+            for (int k = 1; k < n; ++k)
+                for (int q = k; q > 0 && d[leader[q]] < d[leader[q - 1]]; --q) {
+                    const int tmp = leader[q];
+                    leader[q] = leader[q - 1];
+                    leader[q - 1] = tmp;
+                }
+        }
+        __syncthreads();
+        for (int k = tid; k < n; k += TRI_THREADS) {
+            W[mat * n + k] = d[leader[k]];
+            for (int j = 0; j < n; ++j) z[(size_t)j * n + k] = j == leader[k] ? 1.0 : 0.0;
+        }
+        if (tid == 0 && info) info[mat] = 0;
+        return;
+    }
     // ---- eigenvalues: bisection for index k
     const double atol = 2.0 * DBL_EPSILON * onenrm;
     for (int k = tid; k < n; k += TRI_THREADS) {
@@ -324,14 +482,6 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
     // ---- eigenvectors by inverse iteration; a cluster is handled by its leader's thread
     const double eps = DBL_EPSILON;
     const double dtpcrt = sqrt(0.1 / n);
-    if (!(onenrm > 1e3 * DBL_MIN)) {
-        // T = 0 (to underflow): every vector is an eigenvector; return the unit vectors
-        for (int k = tid; k < n; k += TRI_THREADS)
-            for (int j = 0; j < n; ++j) z[(size_t)j * n + k] = j == k ? 1.0 : 0.0;
-        __syncthreads();
-        if (tid == 0 && info) info[mat] = 0;
-        return;
-    }
     for (int k0 = tid; k0 < n; k0 += TRI_THREADS) {
         if (leader[k0] != k0) continue;
         int k1 = k0;
@@ -446,55 +596,175 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
     if (tid == 0 && info) info[mat] = s_fail;
 }
 
-// --------------------------------------------------------------- k_ormtr
-// X = Q Z, Q = H_{n-2} ... H_0; H_i = I - tau_i v_i v_i^H, v_i on rows 0..i with
-// v_i[i] = 1 and v_i[0..i-1] stored in A[0..i-1][i+1].  One CTA per `ch` columns of Z
-// (ch <= ORMTR_COLS, chosen so that the n x ch chunk fits in shared memory).
-__global__ void __launch_bounds__(ORMTR_THREADS)
-k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ TAU, const double* __restrict__ Z,
-        cplx* __restrict__ X, int n, int ch) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* xs = reinterpret_cast<cplx*>(smem_raw);        // [n][ch]
-    cplx* sv = xs + (size_t)n * ch;                       // [ch] tau v^H x per column
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = ORMTR_THREADS / 32;
-    const size_t mat = blockIdx.y;
-    const int col0 = blockIdx.x * ch;
-    const int ncols = min(ch, n - col0);
+// --------------------------------------------------------------- back-transformation
+// X = Q Z with Q = H_{n-2} ... H_0 (H_i = I - tau_i v_i v_i^H, v_i on rows 0..i, v_i[i] = 1,
+// v_i[0..i-1] stored in A[0..i-1][i+1]).  Reflectors are grouped in blocks of ORM_NB
+// consecutive indices i0..i1; a block's product P = H_{i1} ... H_{i0} = I - V T V^H
+// (compact WY form, T lower triangular, built by k_larft) is applied as
+//   X <- X - V (T (V^H X)),
+// blocks in increasing order (LAPACK zlarft / zlarfb, restated).
+static constexpr int ORM_NB = 16;     // reflectors per block
+static constexpr int ORM_RPT = 16;    // rows of the Z chunk held per thread
+
+__device__ __forceinline__ cplx refl_entry(const cplx* __restrict__ a, int n, int i, int r) {
+    // component r of reflector i (zero for i > n-2 padding)
+    if (i > n - 2 || r > i) return mk(0, 0);
+    if (r == i) return mk(1.0, 0.0);
+    return a[(size_t)(i + 1) * n + r];
+}
+
+// T factors of every block of one matrix (one CTA per matrix):
+//   T[k][k] = tau_k,  T[k][q] = -tau_k sum_{l=q}^{k-1} (v_k^H v_l) T[l][q]   (q < k)
+__global__ void __launch_bounds__(256)
+k_larft(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restrict__ Tw, int n) {
+    __shared__ cplx G[ORM_NB][ORM_NB];
+    __shared__ cplx T[ORM_NB][ORM_NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const size_t mat = blockIdx.x;
     const cplx* a = A + mat * (size_t)n * n;
-    const double* z = Z + mat * (size_t)n * n;
-    for (int idx = tid; idx < n * ch; idx += ORMTR_THREADS) {
-        const int r = idx / ch, j = idx % ch;
-        xs[idx] = j < ncols ? mk(z[(size_t)r * n + col0 + j], 0.0) : mk(0, 0);
-    }
-    __syncthreads();
-    for (int i = 0; i <= n - 2; ++i) {
-        const cplx tau = TAU[mat * n + i];
-        if (tau.x == 0.0 && tau.y == 0.0) continue;
-        const cplx* vcol = a + (size_t)(i + 1) * n;
-        for (int j = warp; j < ncols; j += NW) {
+    const cplx* tau = TAU + mat * n;
+    const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
+    for (int j = 0; j < nblk; ++j) {
+        const int i0 = j * ORM_NB;
+        // G[k][l] = v_k^H v_l for l < k: rows 0..i0+l overlap
+        for (int pr = warp; pr < ORM_NB * ORM_NB; pr += 8) {
+            const int k = pr / ORM_NB, l = pr % ORM_NB;
+            if (l >= k) continue;
+            const int ik = i0 + k, il = i0 + l;
             cplx s = mk(0, 0);
-            for (int r = lane; r <= i; r += 32) {
-                const cplx vr = r < i ? vcol[r] : mk(1.0, 0.0);
-                cfmac(s, vr, xs[r * ch + j]);
+            if (ik <= n - 2) {
+                for (int r = lane; r <= il; r += 32) cfmac(s, refl_entry(a, n, ik, r), refl_entry(a, n, il, r));
             }
             s = warp_sum(s);
-            if (lane == 0) sv[j] = cmul(tau, s);
+            if (lane == 0) G[k][l] = s;
         }
         __syncthreads();
-        for (int idx = tid; idx < (i + 1) * ch; idx += ORMTR_THREADS) {
-            const int r = idx / ch, j = idx % ch;
-            if (j < ncols) {
-                const cplx vr = r < i ? vcol[r] : mk(1.0, 0.0);
-                xs[idx] = csub(xs[idx], cmul(vr, sv[j]));
+        if (warp == 0) {
+            for (int k = 0; k < ORM_NB; ++k) {
+                const int ik = i0 + k;
+                const cplx tk = ik <= n - 2 ? tau[ik] : mk(0, 0);
+                if (lane < ORM_NB) {
+                    cplx val = mk(0, 0);
+                    if (lane == k) {
+                        val = tk;
+                    } else if (lane < k) {
+                        cplx s = mk(0, 0);
+                        for (int l = lane; l < k; ++l) cfma(s, G[k][l], T[l][lane]);
+                        val = cscale(cmul(tk, s), -1.0);
+                    }
+                    T[k][lane] = val;
+                }
+                __syncwarp();
             }
         }
         __syncthreads();
+        cplx* out = Tw + (mat * nblk + j) * ORM_NB * ORM_NB;
+        out[threadIdx.x] = T[threadIdx.x / ORM_NB][threadIdx.x % ORM_NB];
+        __syncthreads();
     }
-    cplx* x = X + mat * (size_t)n * n;
-    for (int idx = tid; idx < n * ch; idx += ORMTR_THREADS) {
-        const int j = idx / n, r = idx % n;   // coalesced along r of column col0+j
-        if (j < ncols) x[(size_t)(col0 + j) * n + r] = xs[r * ch + j];
+}
+
+// Apply all blocks to a chunk of CH columns of Z (row-major Z[r*n + col], real) and write
+// the chunk of X (column-major, column = eigenvector).  Thread t owns column t % CH and the
+// rows g + RG*q (g = t / CH, RG = 256/CH, q < ORM_RPT) in registers.
+template <int CH>
+__global__ void __launch_bounds__(256)
+k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* __restrict__ Z,
+        cplx* __restrict__ X, int n) {
+    constexpr int RG = 256 / CH;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx* vs = reinterpret_cast<cplx*>(smem_raw);            // [n][ORM_NB] block of V
+    cplx* ts = vs + (size_t)n * ORM_NB;                       // [ORM_NB][ORM_NB]
+    cplx* wsum = ts + ORM_NB * ORM_NB;                        // [8][ORM_NB][CH]
+    cplx* w2 = wsum + 8 * ORM_NB * CH;                        // [ORM_NB][CH]
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int c = t % CH, g = t / CH;
+    const size_t mat = blockIdx.y;
+    const int col = blockIdx.x * CH + c;
+    const cplx* a = A + mat * (size_t)n * n;
+    const double* z = Z + mat * (size_t)n * n;
+    const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
+    cplx x[ORM_RPT];
+#pragma unroll
+    for (int q = 0; q < ORM_RPT; ++q) {
+        const int r = g + RG * q;
+        x[q] = (r < n && col < n) ? mk(z[(size_t)r * n + col], 0.0) : mk(0, 0);
+    }
+    for (int j = 0; j < nblk; ++j) {
+        const int i0 = j * ORM_NB;
+        const int i1 = min(i0 + ORM_NB - 1, n - 2);
+        __syncthreads();
+        for (int idx = t; idx < (i1 + 1) * ORM_NB; idx += 256) {
+            const int r = idx / ORM_NB, k = idx % ORM_NB;
+            vs[idx] = refl_entry(a, n, i0 + k, r);
+        }
+        ts[t] = Tw[(mat * nblk + j) * ORM_NB * ORM_NB + t];
+        __syncthreads();
+        // partial W = V^H X over this thread's rows
+        cplx wp[ORM_NB];
+#pragma unroll
+        for (int k = 0; k < ORM_NB; ++k) wp[k] = mk(0, 0);
+#pragma unroll
+        for (int q = 0; q < ORM_RPT; ++q) {
+            const int r = g + RG * q;
+            if (r <= i1) {
+                const cplx* vr = vs + r * ORM_NB;
+#pragma unroll
+                for (int k = 0; k < ORM_NB; ++k) cfmac(wp[k], vr[k], x[q]);
+            }
+        }
+        // reduce over the row groups: inside the warp, then across the 8 warps
+#pragma unroll
+        for (int s = CH; s < 32; s <<= 1)
+#pragma unroll
+            for (int k = 0; k < ORM_NB; ++k) wp[k] = cadd(wp[k], shfl_xor(wp[k], s));
+        if (lane < CH)
+#pragma unroll
+            for (int k = 0; k < ORM_NB; ++k) wsum[(warp * ORM_NB + k) * CH + lane] = wp[k];
+        __syncthreads();
+        cplx wk = mk(0, 0);
+        if (t < ORM_NB * CH) {
+            for (int w8 = 0; w8 < 8; ++w8) wk = cadd(wk, wsum[w8 * ORM_NB * CH + t]);
+            wsum[t] = wk;   // W[k][c] at t = k*CH + c (slot of warp 0, already read)
+        }
+        __syncthreads();
+        if (t < ORM_NB * CH) {
+            const int k = t / CH, cc = t % CH;
+            cplx s = mk(0, 0);
+            for (int q2 = 0; q2 <= k; ++q2) cfma(s, ts[k * ORM_NB + q2], wsum[q2 * CH + cc]);
+            w2[t] = s;
+        }
+        __syncthreads();
+        // X -= V W2 on rows <= i1
+        cplx wc[ORM_NB];
+#pragma unroll
+        for (int k = 0; k < ORM_NB; ++k) wc[k] = w2[k * CH + c];
+#pragma unroll
+        for (int q = 0; q < ORM_RPT; ++q) {
+            const int r = g + RG * q;
+            if (r <= i1) {
+                const cplx* vr = vs + r * ORM_NB;
+                cplx s = mk(0, 0);
+#pragma unroll
+                for (int k = 0; k < ORM_NB; ++k) cfma(s, vr[k], wc[k]);
+                x[q] = csub(x[q], s);
+            }
+        }
+    }
+    // write the chunk column-major through shared memory (coalesced along rows)
+    __syncthreads();
+    cplx* xs = vs;   // [CH][n]
+#pragma unroll
+    for (int q = 0; q < ORM_RPT; ++q) {
+        const int r = g + RG * q;
+        if (r < n) xs[(size_t)c * n + r] = x[q];
+    }
+    __syncthreads();
+    cplx* xo = X + mat * (size_t)n * n;
+    const int col0 = blockIdx.x * CH;
+    for (int idx = t; idx < CH * n; idx += 256) {
+        const int cc = idx / n, r = idx % n;
+        if (col0 + cc < n) xo[(size_t)(col0 + cc) * n + r] = xs[idx];
     }
 }
 
@@ -510,7 +780,8 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     cudaStream_t st = ctx->stream;
     const size_t nn = (size_t)n * n;
     // workspace per matrix: D,E (2n), TAU (2n doubles), Z (nn), LU (5nn), X (2nn)
-    const size_t per = (size_t)(4 * n) + nn + 5 * nn + 2 * nn;
+    const size_t tblk = (size_t)((n - 1 + ORM_NB - 1) / ORM_NB) * ORM_NB * ORM_NB;   // T factors
+    const size_t per = (size_t)(4 * n) + nn + 5 * nn + 2 * nn + 2 * tblk;
     // process in chunks bounded by a workspace budget (~8 GB)
     const size_t budget = (size_t)8 << 30;
     size_t chunk = budget / (per * sizeof(double));
@@ -524,30 +795,47 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     double* Zw = reinterpret_cast<double*>(TAUw + chunk * n);
     double* LUw = Zw + chunk * nn;
     cplx* Xw = reinterpret_cast<cplx*>(LUw + 5 * chunk * nn);
+    cplx* Tw = Xw + chunk * nn;
 
-    const size_t smem_trd = 2 * n * sizeof(cplx) + 2 * (HETRD_THREADS / 32) * sizeof(double);
+    // two CTAs per SM: vectors + the resident packed triangle within ~110 KB each
+    const size_t smem_vec = 4 * (size_t)n * sizeof(cplx) + 2 * (HETRD_THREADS / 32) * sizeof(double);
+    const size_t smem_budget = 110 * 1024;
+    int tri_cap = 0;
+    if (smem_budget > smem_vec) tri_cap = (int)((smem_budget - smem_vec) / sizeof(cplx));
+    tri_cap = (int)std::min<size_t>(tri_cap, (size_t)n * (n + 1) / 2);
+    const size_t smem_trd = smem_vec + (size_t)tri_cap * sizeof(cplx);
     const size_t smem_tri = 4 * n * sizeof(double) + n * sizeof(int);
-    int ch = ORMTR_COLS;
-    while (ch > 1 && (size_t)(n + 1) * ch * sizeof(cplx) > 200 * 1024) ch >>= 1;
-    const size_t smem_orm = (size_t)(n + 1) * ch * sizeof(cplx);
+    // back-transform chunk: CH columns per CTA, 256/CH row groups of <= ORM_RPT rows
+    int ch = 16;
+    while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
+    if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;   // n > 4096
+    const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
+    const size_t smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch +
+                             ORM_NB * ch) * sizeof(cplx);
     if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
     RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_trd));
     RLMB_CUDA_TRY(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_orm));
+    auto ormtr = ch == 16 ? k_ormtr<16> : ch == 8 ? k_ormtr<8> : ch == 4 ? k_ormtr<4> : ch == 2 ? k_ormtr<2> : k_ormtr<1>;
+    RLMB_CUDA_TRY(cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_orm));
 
     for (size_t b0 = 0; b0 < (size_t)batch; b0 += chunk) {
         const int nb = (int)std::min(chunk, (size_t)batch - b0);
         cplx* A = reinterpret_cast<cplx*>(d_a) + b0 * nn;
         prof_begin(ctx, "k_hetrd");
-        k_hetrd<<<nb, HETRD_THREADS, smem_trd, st>>>(A, Dw, Ew, TAUw, n);
+        k_hetrd<<<nb, HETRD_THREADS, smem_trd, st>>>(A, Dw, Ew, TAUw, n, tri_cap);
         RLMB_LAUNCHED(ctx);
         prof_begin(ctx, "k_tridiag");
         k_tridiag<<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, d_w + b0 * n, Zw, LUw,
                                                     d_info ? d_info + b0 : nullptr, n);
         RLMB_LAUNCHED(ctx);
+        if (n > 1) {
+            prof_begin(ctx, "k_larft");
+            k_larft<<<nb, 256, 0, st>>>(A, TAUw, Tw, n);
+            RLMB_LAUNCHED(ctx);
+        }
         dim3 g((n + ch - 1) / ch, nb);
         prof_begin(ctx, "k_ormtr");
-        k_ormtr<<<g, ORMTR_THREADS, smem_orm, st>>>(A, TAUw, Zw, Xw, n, ch);
+        ormtr<<<g, 256, smem_orm, st>>>(A, Tw, Zw, Xw, n);
         RLMB_LAUNCHED(ctx);
         RLMB_CUDA_TRY(cudaMemcpyAsync(A, Xw, nb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
     }

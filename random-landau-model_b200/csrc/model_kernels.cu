@@ -516,9 +516,9 @@ k_hlm_links(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int
             cplx* __restrict__ U1, cplx* __restrict__ U2) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int Lxp = lx / Q, N = Lxp * ly;
-    const int dir = blockIdx.z;                       // 0: theta_1 link, 1: theta_2 link
+    const int dir = blockIdx.y;                       // 0: theta_1 link, 1: theta_2 link
     const int kpts = (g + 1) * g;
-    const int job = blockIdx.y, sample = job / kpts, t = job % kpts;
+    const int job = blockIdx.x, sample = job / kpts, t = job % kpts;
     const int t1 = t / g, t2 = t % g;
     if (dir == 0 && t1 == g) return;                  // no theta_1 neighbour of the last line
     const int L = dir == 0 ? Lxp : ly;                // block size
@@ -526,7 +526,7 @@ k_hlm_links(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int
     const int tb2 = dir == 0 ? t2 : (t2 + 1 == g ? 0 : t2 + 1);
     const int tb = tb1 * g + tb2;
     // theta offset (t - t') / g entering D: theta_1 link: -1/g; theta_2 link: (t2 - t2')/g
-    const double shift = dir == 0 ? -1.0 / g : (double)(t2 - (t2 + 1 == g ? 0 : t2 + 1)) / g;
+    const double shift = dir == 0 ? -1.0 / g : (double)(t2 - tb2) / g;
     cplx* S = reinterpret_cast<cplx*>(smem_raw);      // [N][L]: S[a][l], b = partner l of a
     cplx* ub = S + (size_t)N * L;                     // [LINK_STATES][N]
     __shared__ cplx Dtab[64];
@@ -559,42 +559,45 @@ k_hlm_links(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int
     const size_t nn = (size_t)N * N;
     const cplx* Xa = X + ((size_t)sample * kpts + t) * nn;
     const cplx* Xb = X + ((size_t)sample * kpts + tb) * nn;
-    const int s0 = blockIdx.x * LINK_STATES;
-    const int ns = min(LINK_STATES, N - s0);
-    for (int i = threadIdx.x; i < LINK_STATES * N; i += blockDim.x) {
-        const int s = i / N, bidx = i % N;
-        ub[i] = s < ns ? Xb[(size_t)(s0 + s) * N + bidx] : mk(0, 0);
-    }
-    __syncthreads();
-    cplx part[LINK_STATES];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int s0 = 0; s0 < N; s0 += LINK_STATES) {
+        const int ns = min(LINK_STATES, N - s0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < LINK_STATES * N; i += blockDim.x) {
+            const int s = i / N, bidx = i % N;
+            ub[i] = s < ns ? Xb[(size_t)(s0 + s) * N + bidx] : mk(0, 0);
+        }
+        __syncthreads();
+        cplx part[LINK_STATES];
 #pragma unroll
-    for (int s = 0; s < LINK_STATES; ++s) part[s] = mk(0, 0);
-    for (int a = threadIdx.x; a < N; a += blockDim.x) {
-        const int kxa = a / ly, kya = a % ly;
+        for (int s = 0; s < LINK_STATES; ++s) part[s] = mk(0, 0);
+        for (int a = threadIdx.x; a < N; a += blockDim.x) {
+            const int kxa = a / ly, kya = a % ly;
+            const cplx* Sa = S + (size_t)a * L;
 #pragma unroll
-        for (int s = 0; s < LINK_STATES; ++s) {
-            if (s < ns) {
-                cplx y = mk(0, 0);
-                for (int l = 0; l < L; ++l) {
-                    const int b = dir == 0 ? l * ly + kya : kxa * ly + l;
-                    cfma(y, S[(size_t)a * L + l], ub[s * N + b]);
+            for (int s = 0; s < LINK_STATES; ++s) {
+                if (s < ns) {
+                    cplx y = mk(0, 0);
+                    for (int l = 0; l < L; ++l) {
+                        const int b = dir == 0 ? l * ly + kya : kxa * ly + l;
+                        cfma(y, Sa[l], ub[s * N + b]);
+                    }
+                    cfmac(part[s], Xa[(size_t)(s0 + s) * N + a], y);
                 }
-                cfmac(part[s], Xa[(size_t)(s0 + s) * N + a], y);
             }
         }
-    }
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int s = 0; s < LINK_STATES; ++s) {
-        const cplx v = warp_sum(part[s]);
-        if (lane == 0) red[w][s] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < ns) {
-        cplx tot = mk(0, 0);
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot = cadd(tot, red[i][threadIdx.x]);
-        const size_t o = ((size_t)sample * kpts + t) * N + s0 + threadIdx.x;
-        if (dir == 0) U1[o] = tot; else U2[o] = tot;
+        for (int s = 0; s < LINK_STATES; ++s) {
+            const cplx v = warp_sum(part[s]);
+            if (lane == 0) red[w][s] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < ns) {
+            cplx tot = mk(0, 0);
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot = cadd(tot, red[i][threadIdx.x]);
+            const size_t o = ((size_t)sample * kpts + t) * N + s0 + threadIdx.x;
+            if (dir == 0) U1[o] = tot; else U2[o] = tot;
+        }
     }
 }
 
@@ -606,7 +609,7 @@ int launch_hlm_links(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, i
     const size_t smem = ((size_t)N * Lmax + (size_t)LINK_STATES * N) * sizeof(cplx);
     if (smem > 200 * 1024) return RLMB_ERR_ARG;
     RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hlm_links, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((N + LINK_STATES - 1) / LINK_STATES, nsamples * (g + 1) * g, 2);
+    dim3 grid(nsamples * (g + 1) * g, 2);
     prof_begin(ctx, "k_hlm_links");
     k_hlm_links<<<grid, 256, smem, ctx->stream>>>(hb, X, lx, ly, Q, g, U1, U2);
     RLMB_LAUNCHED(ctx);

@@ -80,6 +80,11 @@ def lib():
 
 
 def _check(rc, what):
+    if rc > 0:
+        # positive status: number of matrices whose inverse iteration did not converge
+        import warnings
+        warnings.warn(f"{what}: eigenvectors of {rc} matrices did not converge")
+        return rc
     if rc != 0:
         msg = lib().rlmb_status_string(rc).decode()
         raise RlmbError(f"{what} failed with status {rc}: {msg}")
@@ -139,6 +144,7 @@ class Context:
         if not torch.cuda.is_available():
             raise RlmbError("no CUDA device: the library has no CPU path")
         self.device = device
+        self.last_failures = 0
         h = ctypes.c_void_p()
         _check(lib().rlmb_create(ctypes.byref(h), device), "rlmb_create")
         self.h = h
@@ -282,9 +288,10 @@ class Context:
         e = np.zeros((n_samples, n_phi))
         c = np.zeros((n_samples, n_phi))
         self.sync_stream()
-        _check(lib().rlmb_rlm_mesh_solve(self.h, n_phi, quanta_concentration, impurity_concentration,
-                                         n_mesh, seed, sample0, n_samples, _dp(e), _dp(c)),
-               "rlmb_rlm_mesh_solve")
+        rc = lib().rlmb_rlm_mesh_solve(self.h, n_phi, quanta_concentration, impurity_concentration,
+                                       n_mesh, seed, sample0, n_samples, _dp(e), _dp(c))
+        self.last_failures = max(rc, 0)
+        _check(rc, "rlmb_rlm_mesh_solve")
         return e, c
 
     def hlm_mesh_solve(self, lx, ly, Q, band, n_mesh, potentials):
@@ -294,12 +301,14 @@ class Context:
         e = np.zeros((ns, n_phi))
         c = np.zeros((ns, n_phi))
         self.sync_stream()
-        _check(lib().rlmb_hlm_mesh_solve(self.h, lx, ly, Q, band, n_mesh, _dp(potentials), ns,
-                                         _dp(e), _dp(c)), "rlmb_hlm_mesh_solve")
+        rc = lib().rlmb_hlm_mesh_solve(self.h, lx, ly, Q, band, n_mesh, _dp(potentials), ns, _dp(e), _dp(c))
+        self.last_failures = max(rc, 0)
+        _check(rc, "rlmb_hlm_mesh_solve")
         return e, c
 
     def hlm_mesh_solve_device(self, lx, ly, Q, band, n_mesh, d_potentials, d_energies, d_chern):
         self.sync_stream()
-        _check(lib().rlmb_hlm_mesh_solve_device(self.h, lx, ly, Q, band, n_mesh, _ptr(d_potentials),
-                                                d_potentials.shape[0], _ptr(d_energies), _ptr(d_chern)),
-               "rlmb_hlm_mesh_solve_device")
+        rc = lib().rlmb_hlm_mesh_solve_device(self.h, lx, ly, Q, band, n_mesh, _ptr(d_potentials),
+                                              d_potentials.shape[0], _ptr(d_energies), _ptr(d_chern))
+        self.last_failures = max(rc, 0)
+        _check(rc, "rlmb_hlm_mesh_solve_device")

@@ -114,8 +114,10 @@ def rlm_reference(n_phi, qc, ic, g, n_sample, seed, threads=8, keep_kpoints=()):
     return out
 
 
-def hlm_reference(lx, ly, Q, band, g, n_sample, seed, threads=8, keep_basis=()):
-    """Per-sample loop of hlm/main_hlm_cpu.cpp:354-475 over the reference's functions."""
+def hlm_reference(lx, ly, Q, band, g, n_sample, seed, threads=8, keep_basis=(), only=None,
+                  keep_mesh=True):
+    """Per-sample loop of hlm/main_hlm_cpu.cpp:354-475 over the reference's functions
+    (`only`: the subset of sample indices to solve; the potentials stream covers them all)."""
     lib = hlm_lib()
     n_sites = lx * ly
     n_phi = n_sites // Q
@@ -129,7 +131,7 @@ def hlm_reference(lx, ly, Q, band, g, n_sample, seed, threads=8, keep_basis=()):
         lib.ref_hlm_wfs_ktheta(lx, ly, Q, band, g, t1, t2, ptr(w))
         out[f"basis_{t1}_{t2}"] = w
     E_all, C_all, emesh = [], [], []
-    for n in range(n_sample):
+    for n in (range(n_sample) if only is None else only):
         wf = np.zeros(2 * (g + 1) * dim_wfs, np.complex128)
         et = np.zeros((g + 1) * n_phi)
         ct = np.zeros(g * n_phi)
@@ -153,8 +155,30 @@ def hlm_reference(lx, ly, Q, band, g, n_sample, seed, threads=8, keep_basis=()):
         E_all.append(energy)
         C_all.append(chern)
         emesh.append(em)
-    out.update(energies=np.array(E_all), chern=np.array(C_all), energies_mesh=np.array(emesh))
+    out.update(energies=np.array(E_all), chern=np.array(C_all))
+    if keep_mesh:
+        out["energies_mesh"] = np.array(emesh)
+    if only is not None:
+        out["samples"] = np.array(only)
+        out["potentials"] = pots[list(only)]
     return out
+
+
+def full_size(which):
+    """Full-size fixtures at the benchmark geometries (final energies and Chern numbers)."""
+    if which == "hlm":
+        # the benchmarked hlm configuration (48 x 16, q=3, band 0, g=32, seed 1): samples 0, 5, 22
+        # (5 and 22 are samples whose per-state FHS Chern numbers do not sum to 1)
+        h = hlm_reference(48, 16, 3, 0, 32, 23, 1, only=[0, 5, 22], keep_mesh=False)
+        np.savez_compressed(os.path.join(HERE, "hlm_48x16_q3_b0_g32_s1_full.npz"), **h)
+    if which == "rlm":
+        # rlm n_phi = 512 (g=16) and the finite-size-scaling sizes, sample 0 of seed 1
+        for n_phi in (64, 128, 192, 256, 384, 512):
+            r = rlm_reference(n_phi, 1.0, 16.0, 16, 1, 1)
+            keep = ("n_phi", "qc", "ic", "n_mesh", "n_sample", "seed", "impurity_num", "off_head",
+                    "energies", "chern", "chern_raw")
+            np.savez_compressed(os.path.join(HERE, f"rlm_n{n_phi}_g16_c1_s1_full.npz"),
+                                **{k: v for k, v in r.items() if k in keep})
 
 
 def run_program(args, workdir):
@@ -212,4 +236,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "--full":
+        for w in sys.argv[2:] or ["hlm", "rlm"]:
+            full_size(w)
+    else:
+        main()
