@@ -27,6 +27,7 @@ extern "C" {
 #define RLMB_ERR_CUDA -2
 #define RLMB_ERR_ALLOC -3
 #define RLMB_ERR_NO_DEVICE -4
+#define RLMB_ERR_TOO_LARGE -5
 
 typedef struct rlmb_context rlmb_context;
 
@@ -63,6 +64,21 @@ int rlmb_probe_fp64_peak(rlmb_context* ctx, double* tflops);
 int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch, int* d_info);
 /* Host-pointer form of the same call (copies in and out): the drop-in for mkl_heevd. */
 int rlmb_heevd_host(rlmb_context* ctx, double* h_a, double* h_w, int n, int batch);
+
+/* Allocation-free form of rlmb_heevd_batched; it has no counterpart in the reference.
+ * It is for callers that cannot allocate device memory: processes whose device memory is
+ * already reserved in full by another allocator (a framework's caching pool, a job's fixed
+ * memory budget) and callers that must not take cudaMalloc/cudaFree's implicit device
+ * synchronisation mid-run.  Same layout, arguments and results as rlmb_heevd_batched; no
+ * context, work is queued on `stream` (a cudaStream_t, 0 = legacy default stream).
+ * Scratch is a fixed file-scope device array of RLMB_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading the library holds until exit; a matrix order whose scratch does not fit
+ * (n > 721) returns RLMB_ERR_TOO_LARGE, larger batches are processed in chunks.  The first
+ * call on each device looks the array's device address up (cudaGetSymbolAddress), so make
+ * that first call before any stream capture.  All calls share the array: calls whose GPU
+ * work overlaps in time (other streams or host threads) race. */
+#define RLMB_NOALLOC_SCRATCH_BYTES (32ull << 20)
+int rlmb_heevd_batched_noalloc(double* d_a, double* d_w, int n, int batch, int* d_info, void* stream);
 
 /* ------------------------------------------------------- (a) rlm assembly
  * Disorder-independent coefficient tables, computed on the host exactly as

@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + INCLUDE]
 
-CU_SOURCES = ["heev.cu", "model_kernels.cu", "capi.cu", "profile.cu"]
+CU_SOURCES = ["heev.cu", "model_kernels.cu", "capi.cu", "profile.cu", "heev_noalloc.cu"]
 CPP_SOURCES = ["host_tables.cpp"]
 
 

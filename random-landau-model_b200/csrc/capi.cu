@@ -174,6 +174,7 @@ const char* rlmb_status_string(int status) {
         case RLMB_ERR_CUDA: return "CUDA error";
         case RLMB_ERR_ALLOC: return "device or pinned allocation failed";
         case RLMB_ERR_NO_DEVICE: return "no CUDA device";
+        case RLMB_ERR_TOO_LARGE: return "matrix order exceeds the allocation-free scratch limit";
         default: return status > 0 ? "eigenvectors did not converge for some matrices" : "unknown status";
     }
 }

@@ -768,6 +768,57 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
     }
 }
 
+// Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch.
+size_t heev_scratch_bytes_per_matrix(int n) {
+    const size_t nn = (size_t)n * n;
+    const size_t tblk = (size_t)((n - 1 + ORM_NB - 1) / ORM_NB) * ORM_NB * ORM_NB;
+    return ((size_t)(4 * n) + 8 * nn + 2 * tblk) * sizeof(double);
+}
+
+// The kernel sequence of rlmb_heevd_batched for nb matrices of order n on caller-provided
+// scratch of nb * heev_scratch_bytes_per_matrix(n) bytes (no allocation).  Every scratch
+// region is written by a kernel before any kernel reads it.
+int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n, int nb,
+                          void* scratch, long long* launches) {
+    const size_t nn = (size_t)n * n;
+    const size_t tblk = (size_t)((n - 1 + ORM_NB - 1) / ORM_NB) * ORM_NB * ORM_NB;
+    double* Dw = static_cast<double*>(scratch);
+    double* Ew = Dw + (size_t)nb * n;
+    cplx* TAUw = reinterpret_cast<cplx*>(Ew + (size_t)nb * n);
+    double* Zw = reinterpret_cast<double*>(TAUw + (size_t)nb * n);
+    double* LUw = Zw + (size_t)nb * nn;
+    cplx* Xw = reinterpret_cast<cplx*>(LUw + 5 * (size_t)nb * nn);
+    cplx* Tw = Xw + (size_t)nb * nn;
+    (void)tblk;
+    const size_t smem_vec = 4 * (size_t)n * sizeof(cplx) + 2 * (HETRD_THREADS / 32) * sizeof(double);
+    const size_t smem_budget = 110 * 1024;
+    int tri_cap = 0;
+    if (smem_budget > smem_vec) tri_cap = (int)((smem_budget - smem_vec) / sizeof(cplx));
+    tri_cap = (int)std::min<size_t>(tri_cap, (size_t)n * (n + 1) / 2);
+    const size_t smem_trd = smem_vec + (size_t)tri_cap * sizeof(cplx);
+    const size_t smem_tri = 4 * n * sizeof(double) + n * sizeof(int);
+    int ch = 16;
+    while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
+    if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;
+    const size_t smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch +
+                             ORM_NB * ch) * sizeof(cplx);
+    if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
+    auto ormtr = ch == 16 ? k_ormtr<16> : ch == 8 ? k_ormtr<8> : ch == 4 ? k_ormtr<4> : ch == 2 ? k_ormtr<2> : k_ormtr<1>;
+    if (cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_trd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri) != cudaSuccess ||
+        cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_orm) != cudaSuccess)
+        return RLMB_ERR_CUDA;
+    k_hetrd<<<nb, HETRD_THREADS, smem_trd, st>>>(A, Dw, Ew, TAUw, n, tri_cap);
+    k_tridiag<<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+    if (n > 1) k_larft<<<nb, 256, 0, st>>>(A, TAUw, Tw, n);
+    ormtr<<<dim3((n + ch - 1) / ch, nb), 256, smem_orm, st>>>(A, Tw, Zw, Xw, n);
+    *launches += n > 1 ? 4 : 3;
+    if (cudaGetLastError() != cudaSuccess) return RLMB_ERR_CUDA;
+    if (cudaMemcpyAsync(A, Xw, nb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return RLMB_ERR_CUDA;
+    return RLMB_OK;
+}
+
 }  // namespace rlmb
 
 using namespace rlmb;

@@ -1,0 +1,84 @@
+"""The allocation-free eigensolver entry point, through the C ABI.
+
+rlmb_heevd_batched_noalloc serves callers that cannot allocate device memory (device
+memory already reserved in full by another allocator, or no tolerance for cudaMalloc's
+implicit synchronisation mid-run): its scratch is a fixed file-scope device array.  Its
+results must match rlmb_heevd_batched's, call after call, since every call reuses the same
+array.  This file is collected last so that a failure here leaves the other tests run.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+# the eigensolver tolerances of tests/test_gpu_parity.py
+EIG_TOL = 1e-12
+VEC_TOL = 1e-9
+
+
+def _hermitian_batch(rng, batch, n):
+    a = rng.normal(size=(batch, n, n)) + 1j * rng.normal(size=(batch, n, n))
+    return np.ascontiguousarray(a + np.conj(np.transpose(a, (0, 2, 1))))
+
+
+def _run_batched(ctx, a0):
+    a = torch.tensor(a0, device="cuda")
+    w = ctx.heevd(a)
+    torch.cuda.synchronize()
+    return w.cpu().numpy(), a.cpu().numpy()
+
+
+def _run_noalloc(lib, a0):
+    a = torch.tensor(a0, device="cuda")
+    batch, n = a0.shape[0], a0.shape[-1]
+    w = torch.empty((batch, n), dtype=torch.float64, device="cuda")
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib.rlmb_heevd_batched_noalloc(ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(w.data_ptr()), n,
+                                        batch, ctypes.c_void_p(info.data_ptr()), ctypes.c_void_p(stream))
+    assert rc == 0, lib.rlmb_status_string(rc)
+    torch.cuda.synchronize()
+    assert int(info.abs().sum()) == 0
+    return w.cpu().numpy(), a.cpu().numpy()
+
+
+def _same(wa, Xa, wb, Xb):
+    scale = np.abs(wa).max()
+    assert np.abs(wa - wb).max() <= EIG_TOL * scale
+    # eigenvectors agree up to a phase each (rows are eigenvectors)
+    ov = np.abs(np.einsum("bkr,bkr->bk", np.conj(Xa), Xb))
+    assert np.abs(ov - 1).max() < VEC_TOL
+
+
+@pytest.mark.parametrize("n,batch", [(48, 5), (256, 19)])
+def test_noalloc_matches_batched_twice(n, batch):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import rlmb
+    lib = rlmb.lib()
+    ctx = rlmb.Context(0)
+    rng = np.random.default_rng(n)
+    for call in range(2):
+        a0 = _hermitian_batch(rng, batch, n)
+        wb, Xb = _run_batched(ctx, a0)
+        wn, Xn = _run_noalloc(lib, a0)
+        _same(wb, Xb, wn, Xn)
+    ctx.close()
+
+
+def test_noalloc_rejects_orders_beyond_its_scratch():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import rlmb
+    lib = rlmb.lib()
+    n = 722
+    a = torch.zeros((1, n, n), dtype=torch.complex128, device="cuda")
+    w = torch.zeros((1, n), dtype=torch.float64, device="cuda")
+    rc = lib.rlmb_heevd_batched_noalloc(ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(w.data_ptr()), n, 1,
+                                        None, None)
+    assert rc == -5
+    assert b"scratch limit" in lib.rlmb_status_string(rc)
