@@ -24,7 +24,6 @@
 
 namespace rlmb {
 
-static constexpr int HETRD_THREADS = 256;   // 8 warps
 static constexpr int ORMTR_COLS = 16;       // Z columns per back-transform CTA
 static constexpr int ORMTR_THREADS = 256;
 
@@ -124,67 +123,64 @@ struct SharedStore {
 // warps: applies the rank-2 update A -= v w^H + w v^H of the previous reflector (if upd)
 // and accumulates pn += A' vn for the next one (if acc), reading and writing every
 // stored element once.  All 32 loads of a tile are issued before any of its stores.
-template <class S>
+template <int NT, class S>
 __device__ __forceinline__ void fused_pass(S st, int m, const cplx* __restrict__ v,
                                            const cplx* __restrict__ w, bool upd,
                                            const cplx* __restrict__ vn, bool acc, cplx* pn) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = HETRD_THREADS / 32;
+    constexpr int NW = NT / 32;
     const int nb = (m + 31) / 32;
-    const int ntiles = nb * (nb + 1) / 2;
-    for (int t = warp; t < ntiles; t += NW) {
+    const int nitems = nb * (nb + 1);   // two 16-column halves per 32x32 tile
+    for (int it = warp; it < nitems; it += NW) {
         int R, C;
-        tile_of(t, R, C);
+        tile_of(it >> 1, R, C);
+        const int c0 = C * 32 + 16 * (it & 1);
+        if (c0 >= m) continue;
         const int r = R * 32 + lane;
         const bool rin = r < m;
         const cplx vr = rin ? v[r] : mk(0, 0);
         const cplx wr = rin ? w[r] : mk(0, 0);
         const cplx vnr = rin ? vn[r] : mk(0, 0);
         cplx rowacc = mk(0, 0);
+        cplx e[16];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int c0 = C * 32 + 16 * h;
-            if (c0 >= m) break;
-            cplx e[16];
+        for (int j = 0; j < 16; ++j) {
+            const int cc = c0 + j;
+            e[j] = (rin && cc < m && r <= cc) ? *st.at(r, cc) : mk(0, 0);
+        }
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int cc = c0 + j;
-                e[j] = (rin && cc < m && r <= cc) ? *st.at(r, cc) : mk(0, 0);
-            }
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int cc = c0 + j;
-                const bool valid = rin && cc < m && r <= cc;
-                cplx x = e[j];
-                if (upd) {
-                    const cplx vc = cc < m ? v[cc] : mk(0, 0);
-                    const cplx wc = cc < m ? w[cc] : mk(0, 0);
-                    cplx u = cmul(vr, cconj(wc));
-                    cfma(u, wr, cconj(vc));
-                    x = csub(x, u);
-                    if (r == cc) x.y = 0.0;
-                    if (valid) *st.at(r, cc) = x;
-                }
-                if (acc) {
-                    const cplx vnc = cc < m ? vn[cc] : mk(0, 0);
-                    if (!valid) {
-                        e[j] = mk(0, 0);
-                    } else if (r == cc) {
-                        rowacc = cadd(rowacc, cscale(vnc, x.x));
-                        e[j] = mk(0, 0);
-                    } else {
-                        cfma(rowacc, x, vnc);
-                        e[j] = cmulc(x, vnr);   // column partial: conj(A'[r][cc]) vn[r]
-                    }
-                }
+        for (int j = 0; j < 16; ++j) {
+            const int cc = c0 + j;
+            const bool valid = rin && cc < m && r <= cc;
+            cplx x = e[j];
+            if (upd) {
+                const cplx vc = cc < m ? v[cc] : mk(0, 0);
+                const cplx wc = cc < m ? w[cc] : mk(0, 0);
+                cplx u = cmul(vr, cconj(wc));
+                cfma(u, wr, cconj(vc));
+                x = csub(x, u);
+                if (r == cc) x.y = 0.0;
+                if (valid) *st.at(r, cc) = x;
             }
             if (acc) {
-                const cplx cs = transpose_reduce16(e);
-                const int cl = c0 + (lane & 15);
-                if (lane < 16 && cl < m) smem_atomic_add(&pn[cl], cs);
+                const cplx vnc = cc < m ? vn[cc] : mk(0, 0);
+                if (!valid) {
+                    e[j] = mk(0, 0);
+                } else if (r == cc) {
+                    rowacc = cadd(rowacc, cscale(vnc, x.x));
+                    e[j] = mk(0, 0);
+                } else {
+                    cfma(rowacc, x, vnc);
+                    e[j] = cmulc(x, vnr);   // column partial: conj(A'[r][cc]) vn[r]
+                }
             }
         }
-        if (acc && rin) smem_atomic_add(&pn[r], rowacc);
+        if (acc) {
+            const cplx cs = transpose_reduce16(e);
+            const int cl = c0 + (lane & 15);
+            if (lane < 16 && cl < m) smem_atomic_add(&pn[cl], cs);
+            if (rin) smem_atomic_add(&pn[r], rowacc);
+        }
     }
 }
 
@@ -212,7 +208,8 @@ __device__ __forceinline__ void reflector(const cplx alpha, double xnorm2, doubl
 // reflector of step c-1 (its entry c-1 is 1 and not stored), D/E the tridiagonal and TAU
 // the reflector scalars.  The leading block moves into shared memory once its packed
 // upper triangle fits in `tri_cap` elements.
-__global__ void __launch_bounds__(HETRD_THREADS, 2)
+template <int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 4)
 k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
         cplx* __restrict__ TAU, int n, int tri_cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -221,7 +218,7 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
     cplx* vn = w + n;                               // [n] next reflector / column buffer
     cplx* pn = vn + n;                              // [n] A' vn accumulator
     double* red = reinterpret_cast<double*>(pn + n);  // [2*warps]
-    cplx* tri = reinterpret_cast<cplx*>(red + 2 * (HETRD_THREADS / 32));   // packed triangle
+    cplx* tri = reinterpret_cast<cplx*>(red + 2 * (NT / 32));   // packed triangle
     const int tid = threadIdx.x;
     const size_t mat = blockIdx.x;
     GlobalStore gs{A + mat * (size_t)n * n, n};
@@ -242,23 +239,23 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
     {
         const int i = n - 2;
         double part = 0.0;
-        for (int r = tid; r <= i + 1; r += HETRD_THREADS) {
+        for (int r = tid; r <= i + 1; r += NT) {
             const cplx x = *gs.at(r, i + 1);
             vn[r] = x;
             if (r < i) part += cabs2(x);
         }
-        const double xn2 = block_sum<HETRD_THREADS>(part, red);
+        const double xn2 = block_sum<NT>(part, red);
         double beta;
         cplx tau, scal;
         reflector(vn[i], xn2, beta, tau, scal);
         const bool act = !(tau.x == 0.0 && tau.y == 0.0);
         __syncthreads();
-        for (int r = tid; r < i; r += HETRD_THREADS) {
+        for (int r = tid; r < i; r += NT) {
             const cplx x = act ? cmul(scal, vn[r]) : vn[r];
             v[r] = x;
             *gs.at(r, i + 1) = x;
         }
-        for (int r = tid; r < n; r += HETRD_THREADS) {
+        for (int r = tid; r < n; r += NT) {
             w[r] = mk(0, 0);
             pn[r] = mk(0, 0);
         }
@@ -270,17 +267,17 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
             tt[i] = tau;
         }
         __syncthreads();
-        fused_pass(gs, i + 1, v, w, false, v, act, pn);
+        fused_pass<NT>(gs, i + 1, v, w, false, v, act, pn);
         __syncthreads();
         cplx dpart = mk(0, 0);
-        for (int r = tid; r <= i; r += HETRD_THREADS) {
+        for (int r = tid; r <= i; r += NT) {
             const cplx x = cmul(tau, pn[r]);
             pn[r] = x;
             cfmac(dpart, x, v[r]);
         }
-        const cplx xv = block_sum<HETRD_THREADS>(dpart, red);
+        const cplx xv = block_sum<NT>(dpart, red);
         const cplx al = cscale(cmul(tau, xv), -0.5);
-        for (int r = tid; r <= i; r += HETRD_THREADS) w[r] = cadd(pn[r], cmul(al, v[r]));
+        for (int r = tid; r <= i; r += NT) w[r] = cadd(pn[r], cmul(al, v[r]));
         __syncthreads();
     }
     // -- main loop: v, w belong to step i (column i+1 done); finish column i, build the
@@ -289,14 +286,14 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
         if (!resident && (i + 1) * (i + 2) / 2 <= tri_cap) {
             // move the leading (i+1)x(i+1) upper triangle into shared memory
             for (int c = 0; c <= i; ++c)
-                for (int r = tid; r <= c; r += HETRD_THREADS) *ss.at(r, c) = *gs.at(r, c);
+                for (int r = tid; r <= c; r += NT) *ss.at(r, c) = *gs.at(r, c);
             resident = true;
             __syncthreads();
         }
         // (1) updated column i, rows 0..i
         double part = 0.0;
         const cplx wi = w[i], vi = v[i];
-        for (int r = tid; r <= i; r += HETRD_THREADS) {
+        for (int r = tid; r <= i; r += NT) {
             cplx x = resident ? *ss.at(r, i) : *gs.at(r, i);
             cplx u = cmul(v[r], cconj(wi));
             cfma(u, w[r], cconj(vi));
@@ -305,7 +302,7 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
             if (r < i - 1) part += cabs2(x);
             pn[r] = mk(0, 0);
         }
-        const double xn2 = block_sum<HETRD_THREADS>(part, red);
+        const double xn2 = block_sum<NT>(part, red);
         // (2) reflector of step i-1: alpha = A'[i-1][i], x = A'[0..i-2][i]
         double beta;
         cplx tau, scal;
@@ -313,7 +310,7 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
         const bool act = !(tau.x == 0.0 && tau.y == 0.0);
         __syncthreads();
         if (tid == 0) dd[i] = vn[i].x;
-        for (int r = tid; r < i - 1; r += HETRD_THREADS) {
+        for (int r = tid; r < i - 1; r += NT) {
             const cplx x = act ? cmul(scal, vn[r]) : vn[r];
             vn[r] = x;
             *gs.at(r, i) = x;   // reflector storage stays in global memory
@@ -326,19 +323,19 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
         }
         __syncthreads();
         // (3) fused pass: update [0..i-1]^2 with (v, w), accumulate pn = A' vn
-        if (resident) fused_pass(ss, i, v, w, true, vn, act, pn);
-        else fused_pass(gs, i, v, w, true, vn, act, pn);
+        if (resident) fused_pass<NT>(ss, i, v, w, true, vn, act, pn);
+        else fused_pass<NT>(gs, i, v, w, true, vn, act, pn);
         __syncthreads();
         // (4) w' = tau pn - tau/2 (x^H vn) vn; v <- vn
         cplx dpart = mk(0, 0);
-        for (int r = tid; r < i; r += HETRD_THREADS) {
+        for (int r = tid; r < i; r += NT) {
             const cplx x = cmul(tau, pn[r]);
             pn[r] = x;
             cfmac(dpart, x, vn[r]);
         }
-        const cplx xv = block_sum<HETRD_THREADS>(dpart, red);
+        const cplx xv = block_sum<NT>(dpart, red);
         const cplx al = cscale(cmul(tau, xv), -0.5);
-        for (int r = tid; r < i; r += HETRD_THREADS) {
+        for (int r = tid; r < i; r += NT) {
             w[r] = act ? cadd(pn[r], cmul(al, vn[r])) : mk(0, 0);
             v[r] = vn[r];
         }
@@ -377,6 +374,27 @@ __device__ int sturm_count(const double* __restrict__ d, const double* __restric
     return cnt;
 }
 
+// Sturm count of T - x I together with S = d/dx log|det(T - x I)| = sum_j q_j'/q_j, the
+// pivots' derivative obeying q_j' = -1 + (e_{j-1}^2 / q_{j-1}) (q_{j-1}' / q_{j-1}).
+__device__ int sturm_count_deriv(const double* __restrict__ d, const double* __restrict__ e2, int n,
+                                 double x, double pivmin, double& S) {
+    double q = d[0] - x;
+    if (fabs(q) <= pivmin) q = -pivmin;
+    int cnt = q < 0.0;
+    double t = -1.0 / q;   // q_0'/q_0
+    double sum = t;
+    for (int j = 1; j < n; ++j) {
+        const double r = e2[j - 1] / q;
+        q = d[j] - x - r;
+        if (fabs(q) <= pivmin) q = -pivmin;
+        cnt += q < 0.0;
+        t = (r * t - 1.0) / q;
+        sum += t;
+    }
+    S = sum;
+    return cnt;
+}
+
 // deterministic start vector entries in (-1, 1)
 __device__ __forceinline__ double start_entry(int k, int j) {
     uint32_t h = (uint32_t)k * 0x9E3779B1u ^ ((uint32_t)j * 0x85EBCA77u + 0x165667B1u);
@@ -388,7 +406,62 @@ __device__ __forceinline__ double start_entry(int k, int j) {
     return ((double)h + 0.5) * (2.0 / 4294967296.0) - 1.0;
 }
 
-__global__ void __launch_bounds__(TRI_THREADS)
+// Eigenvector of an isolated eigenvalue x of (d, e) by the twisted factorisation of
+// T - x I (Parlett & Dhillon): forward pivots D+ (the Sturm recurrence) and backward
+// pivots D-, twist index r minimising |gamma_r| = |D+_r + D-_r - (d_r - x)|, then
+// z_r = 1, z_j = -e_j z_{j+1} / D+_j (j < r), z_j = -e_{j-1} z_{j-1} / D-_j (j > r).
+// z (column k of the interleaved Z) first holds D+, dm holds D-.
+__device__ void twisted_vector(const double* __restrict__ d, const double* __restrict__ e,
+                               const double* __restrict__ e2, int n, double x, double pivmin,
+                               double* __restrict__ z, double* __restrict__ dm, int k) {
+    double q = d[0] - x;
+    if (fabs(q) <= pivmin) q = -pivmin;
+    z[k] = q;
+    for (int j = 1; j < n; ++j) {
+        q = d[j] - x - e2[j - 1] / q;
+        if (fabs(q) <= pivmin) q = -pivmin;
+        z[(size_t)j * n + k] = q;
+    }
+    double qb = d[n - 1] - x;
+    if (fabs(qb) <= pivmin) qb = -pivmin;
+    dm[(size_t)(n - 1) * n + k] = qb;
+    int r = n - 1;
+    double gbest = fabs(z[(size_t)(n - 1) * n + k]);   // gamma_{n-1} = D+_{n-1}
+    for (int j = n - 2; j >= 0; --j) {
+        const double aj = d[j] - x;
+        double qn = aj - e2[j] / qb;
+        if (fabs(qn) <= pivmin) qn = -pivmin;
+        qb = qn;
+        dm[(size_t)j * n + k] = qb;
+        const double gam = fabs(z[(size_t)j * n + k] + qb - aj);
+        if (gam < gbest) {
+            gbest = gam;
+            r = j;
+        }
+    }
+    double zz = 1.0, nrm2 = 1.0, big = 1.0;
+    for (int j = r - 1; j >= 0; --j) {
+        zz = -e[j] * zz / z[(size_t)j * n + k];
+        z[(size_t)j * n + k] = zz;
+        nrm2 += zz * zz;
+        if (fabs(zz) > fabs(big)) big = zz;
+    }
+    z[(size_t)r * n + k] = 1.0;
+    zz = 1.0;
+    for (int j = r + 1; j < n; ++j) {
+        zz = -e[j - 1] * zz / dm[(size_t)j * n + k];
+        z[(size_t)j * n + k] = zz;
+        nrm2 += zz * zz;
+        if (fabs(zz) > fabs(big)) big = zz;
+    }
+    double rn = 1.0 / sqrt(nrm2);
+    if (big < 0.0) rn = -rn;
+    for (int j = 0; j < n; ++j) z[(size_t)j * n + k] *= rn;
+}
+
+// PHASE 1 (k_stebz): eigenvalues into W.  PHASE 2 (k_stein): eigenvectors from W.
+template <int PHASE>
+__global__ void __launch_bounds__(TRI_THREADS, 2)
 k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __restrict__ W,
           double* __restrict__ Z, double* __restrict__ LU, int* __restrict__ info, int n) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -439,6 +512,7 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
     const double pivmin = s_pivmin, onenrm = s_onenrm;
     if (!(onenrm > 1e3 * DBL_MIN)) {
         // T = 0 to underflow: eigenvalues are the diagonal (sorted), eigenvectors unit vectors
+        if (PHASE == 2) return;
         if (tid == 0) {
             for (int k = 0; k < n; ++k) leader[k] = k;
             for (int k = 1; k < n; ++k)
@@ -456,20 +530,53 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
         if (tid == 0 && info) info[mat] = 0;
         return;
     }
-    // ---- eigenvalues: bisection for index k
+    // ---- eigenvalue k: bisection on Sturm counts, accelerated by safeguarded Newton steps
+    //      on det(T - x I) once the bracket holds k alone (dstebz bracketing, restated)
+    if (PHASE == 1) {
     const double atol = 2.0 * DBL_EPSILON * onenrm;
     for (int k = tid; k < n; k += TRI_THREADS) {
         double lo = s_gl, hi = s_gu;
-        for (int it = 0; it < 200 && hi - lo > fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi))); ++it) {
-            const double mid = 0.5 * (lo + hi);
-            if (mid <= lo || mid >= hi) break;
-            if (sturm_count(d, e2, n, mid, pivmin) > k) hi = mid; else lo = mid;
+        int clo = 0, chi = n;
+        double x = 0.5 * (lo + hi);
+        double res = x;
+        bool done = false;
+        for (int it = 0; it < 200; ++it) {
+            double S;
+            const int c = sturm_count_deriv(d, e2, n, x, pivmin, S);
+            if (c > k) { hi = x; chi = c; } else { lo = x; clo = c; }
+            const double tol = fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
+            if (hi - lo <= tol) { res = 0.5 * (lo + hi); done = true; break; }
+            double xn = 0.5 * (lo + hi);
+            if (chi - clo == 1 && (it % 4) != 3 && isfinite(S) && S != 0.0) {
+                const double nt = x - 1.0 / S;
+                if (nt > lo && nt < hi) {
+                    if (fabs(nt - x) <= tol) {
+                        // converged step: accept only if Sturm counts bracket index k at nt +- 2 tol
+                        const double a0 = fmax(lo, nt - 2.0 * tol), b0 = fmin(hi, nt + 2.0 * tol);
+                        const int ca = sturm_count(d, e2, n, a0, pivmin);
+                        const int cb = sturm_count(d, e2, n, b0, pivmin);
+                        if (ca <= k && cb > k) { res = nt; done = true; break; }
+                        if (ca > k) { hi = a0; chi = ca; } else { lo = a0; clo = ca; }
+                        if (cb > k) { hi = fmin(hi, b0); chi = cb; } else { lo = fmax(lo, b0); clo = cb; }
+                        xn = 0.5 * (lo + hi);
+                    } else {
+                        xn = nt;
+                    }
+                }
+            }
+            if (xn <= lo || xn >= hi) { res = 0.5 * (lo + hi); done = true; break; }
+            x = xn;
+            res = x;
         }
-        lam[k] = 0.5 * (lo + hi);
+        (void)done;
+        W[mat * n + k] = res;
     }
+    return;
+    }
+    for (int k = tid; k < n; k += TRI_THREADS) lam[k] = W[mat * n + k];
     __syncthreads();
-    // ---- clusters (relative gap 1e-5 of the norm) and eigenvalue output
-    const double ortol = 1e-5 * onenrm;
+    // ---- clusters (relative gap 1e-4 of the norm) and eigenvalue output
+    const double ortol = 1e-4 * onenrm;
     if (tid == 0) {
         int lead = 0;
         for (int k = 0; k < n; ++k) {
@@ -477,15 +584,19 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
             leader[k] = lead;
         }
     }
-    for (int k = tid; k < n; k += TRI_THREADS) W[mat * n + k] = lam[k];
     __syncthreads();
-    // ---- eigenvectors by inverse iteration; a cluster is handled by its leader's thread
+    // ---- eigenvectors: isolated eigenvalues by one twisted solve; clusters by inverse
+    //      iteration with modified Gram-Schmidt, handled by the leader's thread
     const double eps = DBL_EPSILON;
     const double dtpcrt = sqrt(0.1 / n);
     for (int k0 = tid; k0 < n; k0 += TRI_THREADS) {
         if (leader[k0] != k0) continue;
         int k1 = k0;
         while (k1 + 1 < n && leader[k1 + 1] == k0) ++k1;
+        if (k1 == k0) {
+            twisted_vector(d, e, e2, n, lam[k0], pivmin, z, la, k0);
+            continue;
+        }
         double xjm = lam[k0];
         for (int k = k0; k <= k1; ++k) {
             double x = lam[k];
@@ -664,19 +775,49 @@ k_larft(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restri
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Stage block j of V (rows 0..i1, layout [r][k]) and its T factor into shared memory:
+// stored reflector entries by cp.async, the implicit 1 and the zeros below by plain stores.
+__device__ __forceinline__ void stage_block(const cplx* __restrict__ a, const cplx* __restrict__ tsrc,
+                                            cplx* vsb, cplx* tsb, int n, int j) {
+    const int t = threadIdx.x;
+    const int i0 = j * ORM_NB;
+    const int i1 = min(i0 + ORM_NB - 1, n - 2);
+    for (int idx = t; idx < (i1 + 1) * ORM_NB; idx += 256) {
+        const int r = idx / ORM_NB, k = idx % ORM_NB;
+        const int i = i0 + k;
+        if (i <= n - 2 && r < i) cp_async16(&vsb[idx], &a[(size_t)(i + 1) * n + r]);
+        else vsb[idx] = (i <= n - 2 && r == i) ? mk(1.0, 0.0) : mk(0, 0);
+    }
+    cp_async16(&tsb[t], &tsrc[t]);
+    cp_async_commit();
+}
+
 // Apply all blocks to a chunk of CH columns of Z (row-major Z[r*n + col], real) and write
 // the chunk of X (column-major, column = eigenvector).  Thread t owns column t % CH and the
-// rows g + RG*q (g = t / CH, RG = 256/CH, q < ORM_RPT) in registers.
+// rows g + RG*q (g = t / CH, RG = 256/CH, q < ORM_RPT) in registers.  With dbuf the next
+// block's V and T are copied asynchronously while the current block is applied.
 template <int CH>
 __global__ void __launch_bounds__(256)
 k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* __restrict__ Z,
-        cplx* __restrict__ X, int n) {
+        cplx* __restrict__ X, int n, int dbuf) {
     constexpr int RG = 256 / CH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* vs = reinterpret_cast<cplx*>(smem_raw);            // [n][ORM_NB] block of V
-    cplx* ts = vs + (size_t)n * ORM_NB;                       // [ORM_NB][ORM_NB]
-    cplx* wsum = ts + ORM_NB * ORM_NB;                        // [8][ORM_NB][CH]
-    cplx* w2 = wsum + 8 * ORM_NB * CH;                        // [ORM_NB][CH]
+    cplx* vsbuf[2];
+    vsbuf[0] = reinterpret_cast<cplx*>(smem_raw);                    // [n][ORM_NB]
+    vsbuf[1] = dbuf ? vsbuf[0] + (size_t)n * ORM_NB : vsbuf[0];
+    cplx* tsbuf[2];
+    tsbuf[0] = vsbuf[0] + (size_t)(dbuf ? 2 : 1) * n * ORM_NB;       // [ORM_NB][ORM_NB]
+    tsbuf[1] = dbuf ? tsbuf[0] + ORM_NB * ORM_NB : tsbuf[0];
+    cplx* wsum = tsbuf[0] + (size_t)(dbuf ? 2 : 1) * ORM_NB * ORM_NB;   // [8][ORM_NB][CH]
+    cplx* w2 = wsum + 8 * ORM_NB * CH;                                // [ORM_NB][CH]
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int c = t % CH, g = t / CH;
     const size_t mat = blockIdx.y;
@@ -684,22 +825,32 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
     const cplx* a = A + mat * (size_t)n * n;
     const double* z = Z + mat * (size_t)n * n;
     const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
+    const cplx* tw = Tw + mat * (size_t)nblk * ORM_NB * ORM_NB;
     cplx x[ORM_RPT];
 #pragma unroll
     for (int q = 0; q < ORM_RPT; ++q) {
         const int r = g + RG * q;
         x[q] = (r < n && col < n) ? mk(z[(size_t)r * n + col], 0.0) : mk(0, 0);
     }
+    if (dbuf && nblk > 0) stage_block(a, tw, vsbuf[0], tsbuf[0], n, 0);
     for (int j = 0; j < nblk; ++j) {
         const int i0 = j * ORM_NB;
         const int i1 = min(i0 + ORM_NB - 1, n - 2);
-        __syncthreads();
-        for (int idx = t; idx < (i1 + 1) * ORM_NB; idx += 256) {
-            const int r = idx / ORM_NB, k = idx % ORM_NB;
-            vs[idx] = refl_entry(a, n, i0 + k, r);
+        if (dbuf) {
+            if (j + 1 < nblk) {
+                stage_block(a, tw + (size_t)(j + 1) * ORM_NB * ORM_NB, vsbuf[(j + 1) & 1],
+                            tsbuf[(j + 1) & 1], n, j + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+        } else {
+            stage_block(a, tw + (size_t)j * ORM_NB * ORM_NB, vsbuf[0], tsbuf[0], n, j);
+            cp_async_wait<0>();
         }
-        ts[t] = Tw[(mat * nblk + j) * ORM_NB * ORM_NB + t];
         __syncthreads();
+        const cplx* vs = vsbuf[j & 1];
+        const cplx* ts = tsbuf[j & 1];
         // partial W = V^H X over this thread's rows
         cplx wp[ORM_NB];
 #pragma unroll
@@ -715,9 +866,9 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
         }
         // reduce over the row groups: inside the warp, then across the 8 warps
 #pragma unroll
-        for (int s = CH; s < 32; s <<= 1)
+        for (int s2 = CH; s2 < 32; s2 <<= 1)
 #pragma unroll
-            for (int k = 0; k < ORM_NB; ++k) wp[k] = cadd(wp[k], shfl_xor(wp[k], s));
+            for (int k = 0; k < ORM_NB; ++k) wp[k] = cadd(wp[k], shfl_xor(wp[k], s2));
         if (lane < CH)
 #pragma unroll
             for (int k = 0; k < ORM_NB; ++k) wsum[(warp * ORM_NB + k) * CH + lane] = wp[k];
@@ -750,10 +901,10 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
                 x[q] = csub(x[q], s);
             }
         }
+        __syncthreads();
     }
     // write the chunk column-major through shared memory (coalesced along rows)
-    __syncthreads();
-    cplx* xs = vs;   // [CH][n]
+    cplx* xs = vsbuf[0];   // [CH][n]
 #pragma unroll
     for (int q = 0; q < ORM_RPT; ++q) {
         const int r = g + RG * q;
@@ -766,6 +917,40 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
         const int cc = idx / n, r = idx % n;
         if (col0 + cc < n) xo[(size_t)(col0 + cc) * n + r] = xs[idx];
     }
+}
+
+// Launch shape of k_hetrd: small matrices keep their whole triangle in shared memory with
+// 128 threads and several CTAs per SM; larger ones run 512 threads, one CTA per SM, with
+// as much of the leading triangle resident as ~220 KB allows.
+struct HetrdCfg {
+    int nt;
+    int tri_cap;
+    size_t smem;
+};
+static HetrdCfg hetrd_config(int n) {
+    const size_t tri_full = (size_t)n * (n + 1) / 2;
+    const size_t vec128 = 4 * (size_t)n * sizeof(cplx) + 2 * (128 / 32) * sizeof(double);
+    if (vec128 + tri_full * sizeof(cplx) <= 76 * 1024)
+        return {128, (int)tri_full, vec128 + tri_full * sizeof(cplx)};
+    const size_t vec512 = 4 * (size_t)n * sizeof(cplx) + 2 * (512 / 32) * sizeof(double);
+    const size_t budget = 220 * 1024;
+    size_t cap = budget > vec512 ? (budget - vec512) / sizeof(cplx) : 0;
+    cap = std::min(cap, tri_full);
+    return {512, (int)cap, vec512 + cap * sizeof(cplx)};
+}
+static cudaError_t launch_hetrd(const HetrdCfg& c, cudaStream_t st, int nb, cplx* A, double* D, double* E,
+                                cplx* TAU, int n) {
+    if (c.smem > 227 * 1024) return cudaErrorInvalidValue;
+    if (c.nt == 128) {
+        cudaError_t e = cudaFuncSetAttribute(k_hetrd<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
+        if (e != cudaSuccess) return e;
+        k_hetrd<128><<<nb, 128, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(k_hetrd<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
+        if (e != cudaSuccess) return e;
+        k_hetrd<512><<<nb, 512, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
+    }
+    return cudaGetLastError();
 }
 
 // Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch.
@@ -790,29 +975,29 @@ int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n,
     cplx* Xw = reinterpret_cast<cplx*>(LUw + 5 * (size_t)nb * nn);
     cplx* Tw = Xw + (size_t)nb * nn;
     (void)tblk;
-    const size_t smem_vec = 4 * (size_t)n * sizeof(cplx) + 2 * (HETRD_THREADS / 32) * sizeof(double);
-    const size_t smem_budget = 110 * 1024;
-    int tri_cap = 0;
-    if (smem_budget > smem_vec) tri_cap = (int)((smem_budget - smem_vec) / sizeof(cplx));
-    tri_cap = (int)std::min<size_t>(tri_cap, (size_t)n * (n + 1) / 2);
-    const size_t smem_trd = smem_vec + (size_t)tri_cap * sizeof(cplx);
+    const HetrdCfg hc = hetrd_config(n);
+    const size_t smem_trd = hc.smem;
     const size_t smem_tri = 4 * n * sizeof(double) + n * sizeof(int);
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;
-    const size_t smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch +
-                             ORM_NB * ch) * sizeof(cplx);
+    size_t smem_orm = ((size_t)2 * n * ORM_NB + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+    const int dbuf = smem_orm <= 220 * 1024 ? 1 : 0;   // double-buffered V blocks when they fit
+    if (!dbuf)
+        smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
+                   sizeof(cplx);
     if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
     auto ormtr = ch == 16 ? k_ormtr<16> : ch == 8 ? k_ormtr<8> : ch == 4 ? k_ormtr<4> : ch == 2 ? k_ormtr<2> : k_ormtr<1>;
-    if (cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_trd) != cudaSuccess ||
-        cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri) != cudaSuccess ||
+    if (cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri) != cudaSuccess ||
+        cudaFuncSetAttribute(k_tridiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri) != cudaSuccess ||
         cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_orm) != cudaSuccess)
         return RLMB_ERR_CUDA;
-    k_hetrd<<<nb, HETRD_THREADS, smem_trd, st>>>(A, Dw, Ew, TAUw, n, tri_cap);
-    k_tridiag<<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+    if (launch_hetrd(hc, st, nb, A, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
+    k_tridiag<1><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+    k_tridiag<2><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
     if (n > 1) k_larft<<<nb, 256, 0, st>>>(A, TAUw, Tw, n);
-    ormtr<<<dim3((n + ch - 1) / ch, nb), 256, smem_orm, st>>>(A, Tw, Zw, Xw, n);
-    *launches += n > 1 ? 4 : 3;
+    ormtr<<<dim3((n + ch - 1) / ch, nb), 256, smem_orm, st>>>(A, Tw, Zw, Xw, n, dbuf);
+    *launches += n > 1 ? 5 : 4;
     if (cudaGetLastError() != cudaSuccess) return RLMB_ERR_CUDA;
     if (cudaMemcpyAsync(A, Xw, nb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return RLMB_ERR_CUDA;
@@ -848,24 +1033,22 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     cplx* Xw = reinterpret_cast<cplx*>(LUw + 5 * chunk * nn);
     cplx* Tw = Xw + chunk * nn;
 
-    // two CTAs per SM: vectors + the resident packed triangle within ~110 KB each
-    const size_t smem_vec = 4 * (size_t)n * sizeof(cplx) + 2 * (HETRD_THREADS / 32) * sizeof(double);
-    const size_t smem_budget = 110 * 1024;
-    int tri_cap = 0;
-    if (smem_budget > smem_vec) tri_cap = (int)((smem_budget - smem_vec) / sizeof(cplx));
-    tri_cap = (int)std::min<size_t>(tri_cap, (size_t)n * (n + 1) / 2);
-    const size_t smem_trd = smem_vec + (size_t)tri_cap * sizeof(cplx);
+    const HetrdCfg hc = hetrd_config(n);
+    const size_t smem_trd = hc.smem;
     const size_t smem_tri = 4 * n * sizeof(double) + n * sizeof(int);
     // back-transform chunk: CH columns per CTA, 256/CH row groups of <= ORM_RPT rows
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;   // n > 4096
     const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
-    const size_t smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch +
-                             ORM_NB * ch) * sizeof(cplx);
+    size_t smem_orm = ((size_t)2 * n * ORM_NB + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+    const int dbuf = smem_orm <= 220 * 1024 ? 1 : 0;   // double-buffered V blocks when they fit
+    if (!dbuf)
+        smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
+                   sizeof(cplx);
     if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_trd));
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
+    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
+    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_tridiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
     auto ormtr = ch == 16 ? k_ormtr<16> : ch == 8 ? k_ormtr<8> : ch == 4 ? k_ormtr<4> : ch == 2 ? k_ormtr<2> : k_ormtr<1>;
     RLMB_CUDA_TRY(cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_orm));
 
@@ -873,11 +1056,15 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
         const int nb = (int)std::min(chunk, (size_t)batch - b0);
         cplx* A = reinterpret_cast<cplx*>(d_a) + b0 * nn;
         prof_begin(ctx, "k_hetrd");
-        k_hetrd<<<nb, HETRD_THREADS, smem_trd, st>>>(A, Dw, Ew, TAUw, n, tri_cap);
+        RLMB_CUDA_TRY(launch_hetrd(hc, st, nb, A, Dw, Ew, TAUw, n));
         RLMB_LAUNCHED(ctx);
-        prof_begin(ctx, "k_tridiag");
-        k_tridiag<<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, d_w + b0 * n, Zw, LUw,
-                                                    d_info ? d_info + b0 : nullptr, n);
+        prof_begin(ctx, "k_stebz");
+        k_tridiag<1><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, d_w + b0 * n, Zw, LUw,
+                                                       d_info ? d_info + b0 : nullptr, n);
+        RLMB_LAUNCHED(ctx);
+        prof_begin(ctx, "k_stein");
+        k_tridiag<2><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, d_w + b0 * n, Zw, LUw,
+                                                       d_info ? d_info + b0 : nullptr, n);
         RLMB_LAUNCHED(ctx);
         if (n > 1) {
             prof_begin(ctx, "k_larft");
@@ -886,7 +1073,7 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
         }
         dim3 g((n + ch - 1) / ch, nb);
         prof_begin(ctx, "k_ormtr");
-        ormtr<<<g, 256, smem_orm, st>>>(A, Tw, Zw, Xw, n);
+        ormtr<<<g, 256, smem_orm, st>>>(A, Tw, Zw, Xw, n, dbuf);
         RLMB_LAUNCHED(ctx);
         RLMB_CUDA_TRY(cudaMemcpyAsync(A, Xw, nb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
     }

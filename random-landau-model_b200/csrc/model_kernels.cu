@@ -512,7 +512,7 @@ int launch_hlm_project(rlmb_context* ctx, const cplx* hb, const cplx* vt, const 
 static constexpr int LINK_STATES = 16;
 
 __global__ void __launch_bounds__(256)
-k_hlm_links(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int ly, int Q, int g,
+k_hlm_links_generic(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int ly, int Q, int g,
             cplx* __restrict__ U1, cplx* __restrict__ U2) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int Lxp = lx / Q, N = Lxp * ly;
@@ -601,19 +601,139 @@ k_hlm_links(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int
     }
 }
 
-int launch_hlm_links(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,
+int launch_hlm_links_generic(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,
                      int nsamples, cplx* U1, cplx* U2) {
     const int N = lx * ly / Q;
     const int Lmax = std::max(lx / Q, ly);
     if (Lmax > 64) return RLMB_ERR_ARG;
     const size_t smem = ((size_t)N * Lmax + (size_t)LINK_STATES * N) * sizeof(cplx);
     if (smem > 200 * 1024) return RLMB_ERR_ARG;
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hlm_links, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hlm_links_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid(nsamples * (g + 1) * g, 2);
-    prof_begin(ctx, "k_hlm_links");
-    k_hlm_links<<<grid, 256, smem, ctx->stream>>>(hb, X, lx, ly, Q, g, U1, U2);
+    prof_begin(ctx, "k_hlm_links_generic");
+    k_hlm_links_generic<<<grid, 256, smem, ctx->stream>>>(hb, X, lx, ly, Q, g, U1, U2);
     RLMB_LAUNCHED(ctx);
     return RLMB_OK;
+}
+
+// One CTA per (sample, k-point t): both links of t.  S blocks of the two directions are
+// built once in shared memory; thread = state n, which loads one Bloch block of U'(n) into
+// registers and reuses it for the block's L rows (S entries are warp-uniform broadcasts).
+static constexpr int LINK_MAXL = 32;
+
+template <int L>
+__device__ __forceinline__ cplx link_dir(const cplx* __restrict__ S, const cplx* __restrict__ ua,
+                                         const cplx* __restrict__ ub, int nblk, int ly, int dir) {
+    // blocks: dir 1 (theta_2) -> block kx, rows a = kx*ly + i, partners kx*ly + l;
+    //         dir 0 (theta_1) -> block ky, rows a = i*ly + ky, partners l*ly + ky.
+    cplx acc = mk(0, 0);
+    for (int beta = 0; beta < nblk; ++beta) {
+        cplx u[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) u[l] = ub[dir ? beta * ly + l : l * ly + beta];
+#pragma unroll 2
+        for (int i = 0; i < L; ++i) {
+            const int a = dir ? beta * ly + i : i * ly + beta;
+            const cplx* Sa = S + (size_t)a * L;
+            cplx y = mk(0, 0);
+#pragma unroll
+            for (int l = 0; l < L; ++l) cfma(y, Sa[l], u[l]);
+            cfmac(acc, ua[a], y);
+        }
+    }
+    return acc;
+}
+
+__device__ void build_link_S(cplx* S, cplx* Dtab, const cplx* __restrict__ ha, const cplx* __restrict__ hbb,
+                             int N, int L, int ly, int Lxp, int Q, int dir, double shift) {
+    for (int dlt = threadIdx.x; dlt < L; dlt += blockDim.x) {
+        // D_L(dlt + shift) = sum_j e^{i 2pi (dlt + shift) j / L}, dlt = index difference mod L
+        cplx acc = mk(0, 0);
+        for (int j = 0; j < L; ++j) {
+            double sn, cs;
+            sincospi(2.0 * (dlt + shift) * j / L, &sn, &cs);
+            acc = cadd(acc, mk(cs, sn));
+        }
+        Dtab[dlt] = acc;
+    }
+    __syncthreads();
+    const double pref = dir == 0 ? (double)ly : (double)Lxp;
+    for (int idx = threadIdx.x; idx < N * L; idx += blockDim.x) {
+        const int a = idx / L, l = idx % L;
+        const int kxa = a / ly, kya = a % ly;
+        int b, dlt;
+        if (dir == 0) { b = l * ly + kya; dlt = (kxa - l + Lxp) % Lxp; }
+        else { b = kxa * ly + l; dlt = (kya - l + ly) % ly; }
+        cplx ov = mk(0, 0);
+        for (int q = 0; q < Q; ++q) cfmac(ov, ha[(size_t)a * Q + q], hbb[(size_t)b * Q + q]);
+        S[idx] = cscale(cmul(Dtab[dlt], ov), pref);
+    }
+}
+
+template <int L1, int L2>
+__global__ void __launch_bounds__(256)
+k_hlm_links(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int ly, int Q, int g,
+            cplx* __restrict__ U1, cplx* __restrict__ U2) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int Lxp = lx / Q, N = Lxp * ly;
+    const int kpts = (g + 1) * g;
+    const int job = blockIdx.x, sample = job / kpts, t = job % kpts;
+    const int t1 = t / g, t2 = t % g;
+    cplx* S1 = reinterpret_cast<cplx*>(smem_raw);      // theta_1 link: [N][Lxp]
+    cplx* S2 = S1 + (size_t)N * L1;                      // theta_2 link: [N][ly]
+    __shared__ cplx Dtab[LINK_MAXL];
+    const bool has1 = t1 < g;
+    const int t2n = t2 + 1 == g ? 0 : t2 + 1;            // theta_2 = g is the copy of theta_2 = 0
+    const cplx* ha = hb + ((size_t)t1 * (g + 1) + t2) * N * Q;
+    if (has1) {
+        build_link_S(S1, Dtab, ha, hb + ((size_t)(t1 + 1) * (g + 1) + t2) * N * Q, N, L1, ly, Lxp, Q, 0,
+                     -1.0 / g);
+        __syncthreads();
+    }
+    build_link_S(S2, Dtab, ha, hb + ((size_t)t1 * (g + 1) + t2n) * N * Q, N, L2, ly, Lxp, Q, 1,
+                 (double)(t2 - t2n) / g);
+    __syncthreads();
+    const size_t nn = (size_t)N * N;
+    const cplx* Xa = X + ((size_t)sample * kpts + t) * nn;
+    const cplx* Xb1 = X + ((size_t)sample * kpts + (t1 + 1) * g + t2) * nn;
+    const cplx* Xb2 = X + ((size_t)sample * kpts + t1 * g + t2n) * nn;
+    for (int n = threadIdx.x; n < N; n += blockDim.x) {
+        const cplx* ua = Xa + (size_t)n * N;
+        const size_t o = ((size_t)sample * kpts + t) * N + n;
+        if (has1) U1[o] = link_dir<L1>(S1, ua, Xb1 + (size_t)n * N, ly, ly, 0);
+        U2[o] = link_dir<L2>(S2, ua, Xb2 + (size_t)n * N, Lxp, ly, 1);
+    }
+}
+
+template <int L1, int L2>
+static int launch_links_t(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,
+                          int nsamples, cplx* U1, cplx* U2) {
+    const int N = lx * ly / Q;
+    const size_t smem = (size_t)N * (L1 + L2) * sizeof(cplx);
+    if (smem > 220 * 1024) return RLMB_ERR_ARG;
+    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hlm_links<L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    prof_begin(ctx, "k_hlm_links");
+    k_hlm_links<L1, L2><<<nsamples * (g + 1) * g, 256, smem, ctx->stream>>>(hb, X, lx, ly, Q, g, U1, U2);
+    RLMB_LAUNCHED(ctx);
+    return RLMB_OK;
+}
+
+int launch_hlm_links(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,
+                     int nsamples, cplx* U1, cplx* U2) {
+    const int Lxp = lx / Q;
+    // block sizes are compile-time so the U' block lives in registers; others are unsupported
+#define RLMB_LINKS_CASE(A, B) \
+    if (Lxp == A && ly == B) return launch_links_t<A, B>(ctx, hb, X, lx, ly, Q, g, nsamples, U1, U2);
+    RLMB_LINKS_CASE(1, 1) RLMB_LINKS_CASE(1, 2) RLMB_LINKS_CASE(1, 3) RLMB_LINKS_CASE(1, 4)
+    RLMB_LINKS_CASE(2, 2) RLMB_LINKS_CASE(2, 3) RLMB_LINKS_CASE(2, 4) RLMB_LINKS_CASE(2, 6)
+    RLMB_LINKS_CASE(2, 8) RLMB_LINKS_CASE(3, 3) RLMB_LINKS_CASE(3, 6) RLMB_LINKS_CASE(4, 4)
+    RLMB_LINKS_CASE(4, 8) RLMB_LINKS_CASE(8, 8) RLMB_LINKS_CASE(8, 16) RLMB_LINKS_CASE(16, 16)
+    RLMB_LINKS_CASE(16, 8) RLMB_LINKS_CASE(4, 2) RLMB_LINKS_CASE(3, 2) RLMB_LINKS_CASE(6, 6)
+    RLMB_LINKS_CASE(8, 4) RLMB_LINKS_CASE(12, 12) RLMB_LINKS_CASE(16, 32) RLMB_LINKS_CASE(32, 32)
+    RLMB_LINKS_CASE(32, 16)
+#undef RLMB_LINKS_CASE
+    return launch_hlm_links_generic(ctx, hb, X, lx, ly, Q, g, nsamples, U1, U2);
 }
 
 }  // namespace rlmb
