@@ -204,8 +204,11 @@ def _traffic_per_matrix(kernel):
     path = os.path.join(REPO, "profiles", "dram_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel)
-    except (OSError, ValueError):
+            d = json.load(f)
+        if d.get("n") != N_PHI:
+            return None
+        return d["bytes_per_matrix"].get(kernel)
+    except (OSError, ValueError, KeyError):
         return None
 
 
@@ -337,14 +340,36 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def run_probe(args):
+    """One rlmb_heevd_batched call on `batch` random Hermitian matrices of order n (the small
+    case the ncu captures under profiles/ are taken on)."""
+    import numpy as np
+    import torch
+    import rlmb
+    ctx = rlmb.Context(0)
+    rng = np.random.default_rng(0)
+    n, b = args.n, args.batch
+    a0 = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
+    a = torch.tensor(np.ascontiguousarray(a0 + np.conj(np.transpose(a0, (0, 2, 1)))), device="cuda")
+    ctx.heevd(a)
+    torch.cuda.synchronize()
+    print(json.dumps({"probe": "heevd", "n": n, "batch": b, "launches": ctx.launches}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--probe", default=None, choices=["heevd"],
+                    help="run one small eigensolver batch only (for profiler captures)")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=296)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.probe:
+        run_probe(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -374,24 +374,41 @@ __device__ int sturm_count(const double* __restrict__ d, const double* __restric
     return cnt;
 }
 
-// Sturm count of T - x I together with S = d/dx log|det(T - x I)| = sum_j q_j'/q_j, the
-// pivots' derivative obeying q_j' = -1 + (e_{j-1}^2 / q_{j-1}) (q_{j-1}' / q_{j-1}).
-__device__ int sturm_count_deriv(const double* __restrict__ d, const double* __restrict__ e2, int n,
-                                 double x, double pivmin, double& S) {
-    double q = d[0] - x;
-    if (fabs(q) <= pivmin) q = -pivmin;
-    int cnt = q < 0.0;
-    double t = -1.0 / q;   // q_0'/q_0
-    double sum = t;
+// Division-free Sturm count: the leading principal minors p_j of T - x I obey
+//   p_j = (d_j - x) p_{j-1} - e_{j-1}^2 p_{j-2},   p_{-1} = 1,
+// and the number of sign changes along p_{-1}, p_0, ..., p_{n-1} is the number of
+// eigenvalues below x (Sturm).  The pair (p_j, p_{j-1}) is rescaled by exact powers of two
+// to stay in range; a minor that is tiny relative to its predecessor is replaced by
+// -pivmin * p_{j-1}, the same substitution the pivot form q_j = p_j / p_{j-1} uses
+// (dstebz).  The derivatives p_j' ride along for the Newton step ratio = p_{n-1}/p_{n-1}'.
+__device__ __forceinline__ int sturm_poly(const double* __restrict__ d, const double* __restrict__ e2, int n,
+                                          double x, double pivmin, double& ratio) {
+    double pm = 1.0, p = d[0] - x;       // p_{j-1}, p_j
+    double dpm = 0.0, dp = -1.0;          // their derivatives in x
+    if (fabs(p) <= pivmin) p = -pivmin;
+    int cnt = p < 0.0;
     for (int j = 1; j < n; ++j) {
-        const double r = e2[j - 1] / q;
-        q = d[j] - x - r;
-        if (fabs(q) <= pivmin) q = -pivmin;
-        cnt += q < 0.0;
-        t = (r * t - 1.0) / q;
-        sum += t;
+        const double a = d[j] - x;
+        double pn = fma(a, p, -e2[j - 1] * pm);
+        double dpn = fma(a, dp, -fma(e2[j - 1], dpm, p));
+        if (fabs(pn) <= pivmin * fabs(p)) pn = -pivmin * p;
+        cnt += (pn < 0.0) != (p < 0.0);
+        pm = p;
+        dpm = dp;
+        p = pn;
+        dp = dpn;
+        const double big = fmax(fabs(p), fabs(pm));
+        if (big > 0x1p+400 || big < 0x1p-400) {
+            int ex;
+            frexp(big, &ex);
+            const double sc = ldexp(1.0, -ex);
+            p *= sc;
+            pm *= sc;
+            dp *= sc;
+            dpm *= sc;
+        }
     }
-    S = sum;
+    ratio = p / dp;
     return cnt;
 }
 
@@ -410,30 +427,31 @@ __device__ __forceinline__ double start_entry(int k, int j) {
 // T - x I (Parlett & Dhillon): forward pivots D+ (the Sturm recurrence) and backward
 // pivots D-, twist index r minimising |gamma_r| = |D+_r + D-_r - (d_r - x)|, then
 // z_r = 1, z_j = -e_j z_{j+1} / D+_j (j < r), z_j = -e_{j-1} z_{j-1} / D-_j (j > r).
-// z (column k of the interleaved Z) first holds D+, dm holds D-.
+// D+ and D- go to their own scratch columns so the final recurrences can prefetch them.
 __device__ void twisted_vector(const double* __restrict__ d, const double* __restrict__ e,
                                const double* __restrict__ e2, int n, double x, double pivmin,
-                               double* __restrict__ z, double* __restrict__ dm, int k) {
+                               double* __restrict__ z, double* __restrict__ dplus,
+                               double* __restrict__ dminus, int k) {
     double q = d[0] - x;
     if (fabs(q) <= pivmin) q = -pivmin;
-    z[k] = q;
+    dplus[k] = q;
     for (int j = 1; j < n; ++j) {
         q = d[j] - x - e2[j - 1] / q;
         if (fabs(q) <= pivmin) q = -pivmin;
-        z[(size_t)j * n + k] = q;
+        dplus[(size_t)j * n + k] = q;
     }
     double qb = d[n - 1] - x;
     if (fabs(qb) <= pivmin) qb = -pivmin;
-    dm[(size_t)(n - 1) * n + k] = qb;
+    dminus[(size_t)(n - 1) * n + k] = qb;
     int r = n - 1;
-    double gbest = fabs(z[(size_t)(n - 1) * n + k]);   // gamma_{n-1} = D+_{n-1}
+    double gbest = fabs(q);   // gamma_{n-1} = D+_{n-1}
     for (int j = n - 2; j >= 0; --j) {
         const double aj = d[j] - x;
         double qn = aj - e2[j] / qb;
         if (fabs(qn) <= pivmin) qn = -pivmin;
         qb = qn;
-        dm[(size_t)j * n + k] = qb;
-        const double gam = fabs(z[(size_t)j * n + k] + qb - aj);
+        dminus[(size_t)j * n + k] = qb;
+        const double gam = fabs(dplus[(size_t)j * n + k] + qb - aj);
         if (gam < gbest) {
             gbest = gam;
             r = j;
@@ -441,7 +459,7 @@ __device__ void twisted_vector(const double* __restrict__ d, const double* __res
     }
     double zz = 1.0, nrm2 = 1.0, big = 1.0;
     for (int j = r - 1; j >= 0; --j) {
-        zz = -e[j] * zz / z[(size_t)j * n + k];
+        zz = -e[j] * zz / dplus[(size_t)j * n + k];
         z[(size_t)j * n + k] = zz;
         nrm2 += zz * zz;
         if (fabs(zz) > fabs(big)) big = zz;
@@ -449,7 +467,7 @@ __device__ void twisted_vector(const double* __restrict__ d, const double* __res
     z[(size_t)r * n + k] = 1.0;
     zz = 1.0;
     for (int j = r + 1; j < n; ++j) {
-        zz = -e[j - 1] * zz / dm[(size_t)j * n + k];
+        zz = -e[j - 1] * zz / dminus[(size_t)j * n + k];
         z[(size_t)j * n + k] = zz;
         nrm2 += zz * zz;
         if (fabs(zz) > fabs(big)) big = zz;
@@ -541,20 +559,21 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
         double res = x;
         bool done = false;
         for (int it = 0; it < 200; ++it) {
-            double S;
-            const int c = sturm_count_deriv(d, e2, n, x, pivmin, S);
+            double ratio;
+            const int c = sturm_poly(d, e2, n, x, pivmin, ratio);
             if (c > k) { hi = x; chi = c; } else { lo = x; clo = c; }
             const double tol = fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
             if (hi - lo <= tol) { res = 0.5 * (lo + hi); done = true; break; }
             double xn = 0.5 * (lo + hi);
-            if (chi - clo == 1 && (it % 4) != 3 && isfinite(S) && S != 0.0) {
-                const double nt = x - 1.0 / S;
+            if (chi - clo == 1 && (it % 4) != 3 && isfinite(ratio)) {
+                const double nt = x - ratio;
                 if (nt > lo && nt < hi) {
                     if (fabs(nt - x) <= tol) {
                         // converged step: accept only if Sturm counts bracket index k at nt +- 2 tol
                         const double a0 = fmax(lo, nt - 2.0 * tol), b0 = fmin(hi, nt + 2.0 * tol);
-                        const int ca = sturm_count(d, e2, n, a0, pivmin);
-                        const int cb = sturm_count(d, e2, n, b0, pivmin);
+                        double rr;
+                        const int ca = sturm_poly(d, e2, n, a0, pivmin, rr);
+                        const int cb = sturm_poly(d, e2, n, b0, pivmin, rr);
                         if (ca <= k && cb > k) { res = nt; done = true; break; }
                         if (ca > k) { hi = a0; chi = ca; } else { lo = a0; clo = ca; }
                         if (cb > k) { hi = fmin(hi, b0); chi = cb; } else { lo = fmax(lo, b0); clo = cb; }
@@ -594,7 +613,7 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
         int k1 = k0;
         while (k1 + 1 < n && leader[k1 + 1] == k0) ++k1;
         if (k1 == k0) {
-            twisted_vector(d, e, e2, n, lam[k0], pivmin, z, la, k0);
+            twisted_vector(d, e, e2, n, lam[k0], pivmin, z, la, lb, k0);
             continue;
         }
         double xjm = lam[k0];
@@ -716,6 +735,7 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
 // blocks in increasing order (LAPACK zlarft / zlarfb, restated).
 static constexpr int ORM_NB = 16;     // reflectors per block
 static constexpr int ORM_RPT = 16;    // rows of the Z chunk held per thread
+static constexpr int ORM_VS = ORM_NB + 1;   // padded shared-memory row stride of a V block
 
 __device__ __forceinline__ cplx refl_entry(const cplx* __restrict__ a, int n, int i, int r) {
     // component r of reflector i (zero for i > n-2 padding)
@@ -793,8 +813,9 @@ __device__ __forceinline__ void stage_block(const cplx* __restrict__ a, const cp
     for (int idx = t; idx < (i1 + 1) * ORM_NB; idx += 256) {
         const int r = idx / ORM_NB, k = idx % ORM_NB;
         const int i = i0 + k;
-        if (i <= n - 2 && r < i) cp_async16(&vsb[idx], &a[(size_t)(i + 1) * n + r]);
-        else vsb[idx] = (i <= n - 2 && r == i) ? mk(1.0, 0.0) : mk(0, 0);
+        cplx* dst = &vsb[r * ORM_VS + k];
+        if (i <= n - 2 && r < i) cp_async16(dst, &a[(size_t)(i + 1) * n + r]);
+        else *dst = (i <= n - 2 && r == i) ? mk(1.0, 0.0) : mk(0, 0);
     }
     cp_async16(&tsb[t], &tsrc[t]);
     cp_async_commit();
@@ -811,10 +832,10 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
     constexpr int RG = 256 / CH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx* vsbuf[2];
-    vsbuf[0] = reinterpret_cast<cplx*>(smem_raw);                    // [n][ORM_NB]
-    vsbuf[1] = dbuf ? vsbuf[0] + (size_t)n * ORM_NB : vsbuf[0];
+    vsbuf[0] = reinterpret_cast<cplx*>(smem_raw);                    // [n][ORM_VS]
+    vsbuf[1] = dbuf ? vsbuf[0] + (size_t)n * ORM_VS : vsbuf[0];
     cplx* tsbuf[2];
-    tsbuf[0] = vsbuf[0] + (size_t)(dbuf ? 2 : 1) * n * ORM_NB;       // [ORM_NB][ORM_NB]
+    tsbuf[0] = vsbuf[0] + (size_t)(dbuf ? 2 : 1) * n * ORM_VS;       // [ORM_NB][ORM_NB]
     tsbuf[1] = dbuf ? tsbuf[0] + ORM_NB * ORM_NB : tsbuf[0];
     cplx* wsum = tsbuf[0] + (size_t)(dbuf ? 2 : 1) * ORM_NB * ORM_NB;   // [8][ORM_NB][CH]
     cplx* w2 = wsum + 8 * ORM_NB * CH;                                // [ORM_NB][CH]
@@ -859,7 +880,7 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
         for (int q = 0; q < ORM_RPT; ++q) {
             const int r = g + RG * q;
             if (r <= i1) {
-                const cplx* vr = vs + r * ORM_NB;
+                const cplx* vr = vs + r * ORM_VS;
 #pragma unroll
                 for (int k = 0; k < ORM_NB; ++k) cfmac(wp[k], vr[k], x[q]);
             }
@@ -894,7 +915,7 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
         for (int q = 0; q < ORM_RPT; ++q) {
             const int r = g + RG * q;
             if (r <= i1) {
-                const cplx* vr = vs + r * ORM_NB;
+                const cplx* vr = vs + r * ORM_VS;
                 cplx s = mk(0, 0);
 #pragma unroll
                 for (int k = 0; k < ORM_NB; ++k) cfma(s, vr[k], wc[k]);
@@ -981,10 +1002,10 @@ int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n,
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;
-    size_t smem_orm = ((size_t)2 * n * ORM_NB + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+    size_t smem_orm = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
     const int dbuf = smem_orm <= 220 * 1024 ? 1 : 0;   // double-buffered V blocks when they fit
     if (!dbuf)
-        smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
+        smem_orm = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
                    sizeof(cplx);
     if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
     auto ormtr = ch == 16 ? k_ormtr<16> : ch == 8 ? k_ormtr<8> : ch == 4 ? k_ormtr<4> : ch == 2 ? k_ormtr<2> : k_ormtr<1>;
@@ -1041,10 +1062,10 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;   // n > 4096
     const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
-    size_t smem_orm = ((size_t)2 * n * ORM_NB + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+    size_t smem_orm = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
     const int dbuf = smem_orm <= 220 * 1024 ? 1 : 0;   // double-buffered V blocks when they fit
     if (!dbuf)
-        smem_orm = ((size_t)std::max(n * ORM_NB, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
+        smem_orm = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
                    sizeof(cplx);
     if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
     RLMB_CUDA_TRY(cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
