@@ -22,7 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + INCLUDE]
 
-CU_SOURCES = ["heev.cu", "model_kernels.cu", "capi.cu", "profile.cu", "heev_noalloc.cu"]
+CU_SOURCES = ["heev.cu", "model_kernels.cu", "capi.cu", "profile.cu", "heev_noalloc.cu", "diag_wrappers.cu"]
+DRIVERS = {"rlm": "tools/rlm_main.cpp", "hlm": "tools/hlm_main.cpp"}
 CPP_SOURCES = ["host_tables.cpp"]
 
 
@@ -58,6 +59,14 @@ def build(force=False):
         objs.append(o)
     if force or _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
+    os.makedirs(BIN, exist_ok=True)
+    for name, src in DRIVERS.items():
+        s = os.path.join(CSRC, src)
+        exe = os.path.join(BIN, name)
+        deps = [s, LIB, os.path.join(CSRC, "tools", "driver_common.h")]
+        if force or _stale(exe, deps):
+            _run([CXX, "-O2", "-std=c++17", "-I" + INCLUDE, s, "-o", exe, "-L" + os.path.dirname(LIB),
+                  "-lrlmb", "-Wl,-rpath,$ORIGIN/../lib"])
     return LIB
 
 

@@ -1,0 +1,128 @@
+"""The reference-named C++ entry points (include/diag_wrappers_b200.h), called from C++ as
+the reference's own call sites call them (tests/wrappers_check.cpp), against the oracle and
+the reference's golden fixtures."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG_ROOT, REPO, golden
+
+LIBDIR = os.path.join(PKG_ROOT, "lib")
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    if not os.path.exists(os.path.join(LIBDIR, "librlmb.so")):
+        pytest.skip("library not built")
+    exe = str(tmp_path_factory.mktemp("wrap") / "wrappers_check")
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    subprocess.run(["g++", "-O2", "-std=c++17", os.path.join(REPO, "tests", "wrappers_check.cpp"),
+                    "-I" + os.path.join(REPO, "include"), "-I" + os.path.join(cuda, "include"),
+                    "-L" + LIBDIR, "-lrlmb", "-L" + os.path.join(cuda, "lib64"), "-lcudart",
+                    "-Wl,-rpath," + LIBDIR + ":" + os.path.join(cuda, "lib64"), "-o", exe], check=True)
+    return exe
+
+
+def _call(exe, *args):
+    r = subprocess.run([exe] + [str(a) for a in args], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stderr == "", r.stderr     # the wrappers report failures on stderr
+
+
+def test_host_tables_and_disorder_wrappers(harness, tmp_path):
+    d = golden("rlm_n32_g4_c1_s7.npz")
+    n_phi, o, g = int(d["n_phi"]), int(d["off_head"]), int(d["n_mesh"])
+    L = float(np.sqrt(n_phi * float(d["qc"])))
+    out = tmp_path / "t.bin"
+    _call(harness, "tables", out, n_phi, o, g, repr(L))
+    raw = np.fromfile(out, np.complex128)
+    dim = 2 * o + 1
+    assert np.array_equal(raw[:dim * dim], d["coeff_mn"])
+    assert np.array_equal(raw[dim * dim:dim * dim + (g + 1) * dim], d["coeff_m_theta"])
+    assert np.array_equal(raw[dim * dim + (g + 1) * dim:], d["coeff_jm"])
+    nimp = int(d["impurity_num"])
+    _call(harness, "disorder", out, nimp, repr(L), int(d["seed"]), 0)
+    raw = np.fromfile(out, np.float64)
+    assert np.array_equal(raw[:nimp], d["x"][0]) and np.array_equal(raw[2 * nimp:], d["s"][0])
+
+
+def _gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+@pytest.mark.gpu
+def test_mkl_heevd_wrapper(harness, tmp_path):
+    _gpu()
+    rng = np.random.default_rng(5)
+    n = 40
+    a = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    M = (a + a.conj().T) / 2
+    inp = tmp_path / "in.bin"
+    M.T.astype(np.complex128).tofile(inp)          # column-major
+    _call(harness, "heevd", inp, tmp_path / "out.bin", n)
+    raw = np.fromfile(tmp_path / "out.bin", np.float64)
+    w = raw[:n]
+    X = raw[n:].view(np.complex128).reshape(n, n).T   # columns = eigenvectors
+    assert np.abs(w - np.linalg.eigvalsh(M)).max() <= 1e-12 * np.abs(w).max()
+    assert np.linalg.norm(M @ X - X * w) <= 1e-12 * np.linalg.norm(M)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["cusolver", "magma"])
+def test_single_precision_device_wrappers(harness, tmp_path, mode):
+    _gpu()
+    rng = np.random.default_rng(9)
+    n = 33
+    a = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    M = (a + a.conj().T) / 2
+    buf = M.T.astype(np.complex64)            # column-major: buf[c][r] = M[r][c]
+    buf[np.tril_indices(n, -1)] = 99 + 99j     # garbage in the upper triangle: uplo = lower
+    buf.tofile(tmp_path / "in.bin")
+    _call(harness, mode, tmp_path / "in.bin", tmp_path / "out.bin", n)
+    raw = np.fromfile(tmp_path / "out.bin", np.float32)
+    w = raw[:n].astype(np.float64)
+    X = raw[n:].view(np.complex64).reshape(n, n).T.astype(np.complex128)
+    wref = np.linalg.eigvalsh(M.astype(np.complex64).astype(np.complex128))
+    assert np.abs(w - wref).max() <= 1e-5 * np.abs(wref).max()
+    assert np.linalg.norm(M @ X - X * w) <= 1e-5 * np.linalg.norm(M)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["chern", "peer"])
+def test_chern_wrappers_match_reference_layout(harness, tmp_path, mode):
+    _gpu()
+    from oracle import fhs, rlm as orlm
+    d = golden("rlm_n16_g8_c2_s1.npz")
+    p = orlm.RlmParams(16, 1.0, 16.0, 8, 1, 1)
+    X = orlm.run_sample(p, 0, keep=True)["eigvecs"]       # [(g+1), (g+1), N, N]
+    g, N = 8, 16
+    t1 = 3
+    ring = np.empty((2, g + 1, N, N), np.complex128)
+    ring[t1 % 2] = X[t1]
+    ring[1 - t1 % 2] = X[t1 - 1]
+    ring.tofile(tmp_path / "w.bin")
+    _call(harness, mode, tmp_path / "w.bin", tmp_path / "c.bin", N, N, g, t1)
+    got = np.fromfile(tmp_path / "c.bin", np.float64).reshape(N, g)   # [n][m]
+    ref = fhs.line_chern(X[t1 - 1], X[t1]).T
+    cols = range(g) if mode == "chern" else range(1, g, 2)
+    for m in cols:
+        assert np.abs(got[:, m] - ref[:, m]).max() < 1e-10
+    if mode == "peer":
+        assert np.all(got[:, 0::2] == -7.0)      # untouched plaquettes
+    assert d is not None
+
+
+@pytest.mark.gpu
+def test_get_potential_coeff_wrapper(harness, tmp_path):
+    _gpu()
+    d = golden("rlm_n64_g4_c1_s3.npz")
+    nimp, o = int(d["impurity_num"]), int(d["off_head"])
+    dim = 2 * o + 1
+    np.concatenate([d["x"][0], d["y"][0], d["s"][0], d["coeff_mn"].view(np.float64)]).tofile(tmp_path / "i.bin")
+    _call(harness, "vmn", tmp_path / "i.bin", tmp_path / "v.bin", nimp, dim, o)
+    v = np.fromfile(tmp_path / "v.bin", np.complex128)
+    assert np.abs(v - d["v_mn"][0]).max() <= 1e-12 * np.abs(d["v_mn"][0]).max()
