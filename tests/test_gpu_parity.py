@@ -279,3 +279,30 @@ def test_hlm_mesh_solve_matches_reference(ctx, name):
         assert np.abs(e[n] - eref).max() <= 1e-10 * np.abs(eref).max()
         assert np.array_equal(np.rint(c[n]), np.rint(cref))
         assert np.abs(c[n] - cref).max() < 1e-8
+
+
+# ----------------------------------------------------- full-size geometries (reference fixtures)
+def test_hlm_benchmark_geometry_matches_reference(ctx):
+    """hlm 48x16, q=3, band 0, g=32 (the benchmarked configuration): samples 0, 5 and 22 of
+    seed 1, whose per-state Chern sums the reference gives as 1, 2 and 0."""
+    d = golden("hlm_48x16_q3_b0_g32_s1_full.npz")
+    e, c = ctx.hlm_mesh_solve(48, 16, 3, 0, 32, d["potentials"])
+    assert ctx.last_failures == 0
+    for i in range(len(d["samples"])):
+        eref, cref = d["energies"][i], d["chern"][i]
+        assert np.abs(e[i] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[i]), np.rint(cref))
+        assert np.abs(c[i] - cref).max() < 1e-8
+    assert [round(float(x)) for x in c.sum(axis=1)] == [round(float(x)) for x in d["chern"].sum(axis=1)]
+
+
+@pytest.mark.parametrize("n_phi", [64, 128, 192, 256, 384, 512])
+def test_rlm_finite_size_geometries_match_reference(ctx, n_phi):
+    """rlm at the finite-size-scaling sizes (impurity concentration 16, g=16, seed 1, sample 0)."""
+    d = golden(f"rlm_n{n_phi}_g16_c1_s1_full.npz")
+    e, c = ctx.rlm_mesh_solve(n_phi, 1.0, 16.0, 16, 1, 0, 1)
+    assert ctx.last_failures == 0
+    eref, cref = d["energies"][0], d["chern"][0]
+    assert np.abs(e[0] - eref).max() <= 1e-10 * np.abs(eref).max()
+    assert np.array_equal(np.rint(c[0]), np.rint(cref))
+    assert np.abs(c[0] - cref).max() < 1e-8
