@@ -430,19 +430,19 @@ __device__ __forceinline__ double start_entry(int k, int j) {
 // D+ and D- go to their own scratch columns so the final recurrences can prefetch them.
 __device__ void twisted_vector(const double* __restrict__ d, const double* __restrict__ e,
                                const double* __restrict__ e2, int n, double x, double pivmin,
-                               double* __restrict__ z, double* __restrict__ dplus,
-                               double* __restrict__ dminus, int k) {
+                               double* __restrict__ z, int k, double* __restrict__ dplus,
+                               double* __restrict__ dminus, int sc) {
     double q = d[0] - x;
     if (fabs(q) <= pivmin) q = -pivmin;
-    dplus[k] = q;
+    dplus[sc] = q;
     for (int j = 1; j < n; ++j) {
         q = d[j] - x - e2[j - 1] / q;
         if (fabs(q) <= pivmin) q = -pivmin;
-        dplus[(size_t)j * n + k] = q;
+        dplus[(size_t)j * TRI_THREADS + sc] = q;
     }
     double qb = d[n - 1] - x;
     if (fabs(qb) <= pivmin) qb = -pivmin;
-    dminus[(size_t)(n - 1) * n + k] = qb;
+    dminus[(size_t)(n - 1) * TRI_THREADS + sc] = qb;
     int r = n - 1;
     double gbest = fabs(q);   // gamma_{n-1} = D+_{n-1}
     for (int j = n - 2; j >= 0; --j) {
@@ -450,8 +450,8 @@ __device__ void twisted_vector(const double* __restrict__ d, const double* __res
         double qn = aj - e2[j] / qb;
         if (fabs(qn) <= pivmin) qn = -pivmin;
         qb = qn;
-        dminus[(size_t)j * n + k] = qb;
-        const double gam = fabs(dplus[(size_t)j * n + k] + qb - aj);
+        dminus[(size_t)j * TRI_THREADS + sc] = qb;
+        const double gam = fabs(dplus[(size_t)j * TRI_THREADS + sc] + qb - aj);
         if (gam < gbest) {
             gbest = gam;
             r = j;
@@ -459,7 +459,7 @@ __device__ void twisted_vector(const double* __restrict__ d, const double* __res
     }
     double zz = 1.0, nrm2 = 1.0, big = 1.0;
     for (int j = r - 1; j >= 0; --j) {
-        zz = -e[j] * zz / dplus[(size_t)j * n + k];
+        zz = -e[j] * zz / dplus[(size_t)j * TRI_THREADS + sc];
         z[(size_t)j * n + k] = zz;
         nrm2 += zz * zz;
         if (fabs(zz) > fabs(big)) big = zz;
@@ -467,7 +467,7 @@ __device__ void twisted_vector(const double* __restrict__ d, const double* __res
     z[(size_t)r * n + k] = 1.0;
     zz = 1.0;
     for (int j = r + 1; j < n; ++j) {
-        zz = -e[j - 1] * zz / dminus[(size_t)j * n + k];
+        zz = -e[j - 1] * zz / dminus[(size_t)j * TRI_THREADS + sc];
         z[(size_t)j * n + k] = zz;
         nrm2 += zz * zz;
         if (fabs(zz) > fabs(big)) big = zz;
@@ -494,11 +494,15 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
     const size_t mat = blockIdx.x;
     const size_t nn = (size_t)n * n;
     double* z = Z + mat * nn;
-    double* la = LU + mat * 5 * nn;    // a (U main), b (U super1), c2 (U super2), mult, piv
-    double* lb = la + nn;
-    double* lc2 = lb + nn;
-    double* lm = lc2 + nn;
-    double* lp = lm + nn;
+    // per-thread scratch columns (column = thread, stride TRI_THREADS): U diag / super1 /
+    // super2, multipliers and swap flags of the LU of T - x I; the twisted solve uses the
+    // first two as D+ and D-
+    const size_t lus = (size_t)n * TRI_THREADS;
+    double* la = LU + mat * 5 * lus;
+    double* lb = la + lus;
+    double* lc2 = lb + lus;
+    double* lm = lc2 + lus;
+    double* lp = lm + lus;
 
     for (int j = tid; j < n; j += TRI_THREADS) {
         d[j] = D[mat * n + j];
@@ -613,7 +617,7 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
         int k1 = k0;
         while (k1 + 1 < n && leader[k1 + 1] == k0) ++k1;
         if (k1 == k0) {
-            twisted_vector(d, e, e2, n, lam[k0], pivmin, z, la, lb, k0);
+            twisted_vector(d, e, e2, n, lam[k0], pivmin, z, k0, la, lb, tid);
             continue;
         }
         double xjm = lam[k0];
@@ -627,13 +631,13 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
             // LU with partial pivoting of T - x I (dlagtf).  The active row carries
             // (u0, u1) = its entries in columns j, j+1; the row pivoted into position j is
             // stored as U diag / super1 / super2 (la, lb, lc2), the multiplier in lm and
-            // the swap flag in lp, all at [j*n + k].
+            // the swap flag in lp, all at [j*TRI_THREADS + thread] (one column per thread).
             double u0 = d[0] - x, u1 = n > 1 ? e[0] : 0.0;
             for (int j = 0; j < n - 1; ++j) {
                 const double cj = e[j];
                 const double anext = d[j + 1] - x;
                 const double bnext = j + 1 < n - 1 ? e[j + 1] : 0.0;
-                const size_t o = (size_t)j * n + k;
+                const size_t o = (size_t)j * TRI_THREADS + tid;
                 if (fabs(u0) >= fabs(cj)) {
                     const double mult = u0 != 0.0 ? cj / u0 : 0.0;
                     la[o] = u0;
@@ -654,12 +658,12 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
                     u1 = -mult * bnext;
                 }
             }
-            la[(size_t)(n - 1) * n + k] = u0;
-            lb[(size_t)(n - 1) * n + k] = 0.0;
-            lc2[(size_t)(n - 1) * n + k] = 0.0;
+            la[(size_t)(n - 1) * TRI_THREADS + tid] = u0;
+            lb[(size_t)(n - 1) * TRI_THREADS + tid] = 0.0;
+            lc2[(size_t)(n - 1) * TRI_THREADS + tid] = 0.0;
             // tiny pivots are perturbed to +-tolp in the solves (dlagts job = -1)
             double umax = 0.0;
-            for (int j = 0; j < n; ++j) umax = fmax(umax, fabs(la[(size_t)j * n + k]));
+            for (int j = 0; j < n; ++j) umax = fmax(umax, fabs(la[(size_t)j * TRI_THREADS + tid]));
             const double tolp = fmax(eps * fmax(umax, onenrm), DBL_MIN);
             for (int j = 0; j < n; ++j) z[(size_t)j * n + k] = start_entry(k, j);
             int nrmchk = 0;
@@ -668,15 +672,16 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
                 // scale the right-hand side to ||b||_1 = n * onenrm * max(eps, |u_nn|)
                 double b1 = 0.0;
                 for (int j = 0; j < n; ++j) b1 += fabs(z[(size_t)j * n + k]);
-                const double unn = fabs(la[(size_t)(n - 1) * n + k]);
+                const double unn = fabs(la[(size_t)(n - 1) * TRI_THREADS + tid]);
                 const double sc = n * onenrm * fmax(eps, unn) / fmax(b1, DBL_MIN);
                 // forward: y = L^{-1} P b  (the active right-hand side value is carried)
                 double rc = z[k] * sc;
                 for (int j = 0; j < n - 1; ++j) {
                     const size_t o = (size_t)j * n + k;
+                    const size_t ol = (size_t)j * TRI_THREADS + tid;
                     const double bnext = z[(size_t)(j + 1) * n + k] * sc;
-                    const double mult = lm[o];
-                    if (lp[o] != 0.0) {
+                    const double mult = lm[ol];
+                    if (lp[ol] != 0.0) {
                         z[o] = bnext;
                         rc = rc - mult * bnext;
                     } else {
@@ -690,9 +695,10 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
                 double xmax = 0.0;
                 for (int j = n - 1; j >= 0; --j) {
                     const size_t o = (size_t)j * n + k;
-                    double u = la[o];
+                    const size_t ol = (size_t)j * TRI_THREADS + tid;
+                    double u = la[ol];
                     if (fabs(u) < tolp) u = u >= 0.0 ? tolp : -tolp;
-                    const double xj = (z[o] - lb[o] * x1 - lc2[o] * x2) / u;
+                    const double xj = (z[o] - lb[ol] * x1 - lc2[ol] * x2) / u;
                     z[o] = xj;
                     x2 = x1;
                     x1 = xj;
@@ -940,6 +946,196 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
     }
 }
 
+// ------------------------------------------------ back-transformation for large orders
+// For orders whose 16-reflector blocks do not fit the register/shared-memory scheme of
+// k_ormtr, X = Q Z is applied with blocks of BT_NB = 64 reflectors as two tiled complex
+// GEMMs per block (LAPACK zlarfb restated): W' = T (V^H X), then X -= V W'.  X lives in
+// global memory (column-major, column = eigenvector) and is read twice and written once
+// per block.
+static constexpr int BT_NB = 64;
+
+// T factor of block j (reflectors 64j .. 64j+63) of one matrix; grid (blocks, matrices).
+__global__ void __launch_bounds__(256)
+k_larft64(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restrict__ Tw, int n) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx* G = reinterpret_cast<cplx*>(smem_raw);   // [64][64]
+    cplx* T = G + BT_NB * BT_NB;                   // [64][64]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = blockIdx.x;
+    const size_t mat = blockIdx.y;
+    const cplx* a = A + mat * (size_t)n * n;
+    const cplx* tau = TAU + mat * n;
+    const int nblk = (n - 1 + BT_NB - 1) / BT_NB;
+    const int i0 = j * BT_NB;
+    for (int pr = warp; pr < BT_NB * BT_NB; pr += 8) {
+        const int k = pr / BT_NB, l = pr % BT_NB;
+        if (l >= k) continue;
+        const int ik = i0 + k, il = i0 + l;
+        cplx s = mk(0, 0);
+        if (ik <= n - 2)
+            for (int r = lane; r <= il; r += 32) cfmac(s, refl_entry(a, n, ik, r), refl_entry(a, n, il, r));
+        s = warp_sum(s);
+        if (lane == 0) G[k * BT_NB + l] = s;
+    }
+    __syncthreads();
+    for (int k = 0; k < BT_NB; ++k) {
+        const int ik = i0 + k;
+        const cplx tk = ik <= n - 2 ? tau[ik] : mk(0, 0);
+        if (threadIdx.x < BT_NB) {
+            const int q = threadIdx.x;
+            cplx val = mk(0, 0);
+            if (q == k) {
+                val = tk;
+            } else if (q < k) {
+                cplx s = mk(0, 0);
+                for (int l = q; l < k; ++l) cfma(s, G[k * BT_NB + l], T[l * BT_NB + q]);
+                val = cscale(cmul(tk, s), -1.0);
+            }
+            T[k * BT_NB + q] = val;
+        }
+        __syncthreads();
+    }
+    cplx* out = Tw + (mat * nblk + j) * BT_NB * BT_NB;
+    for (int i = threadIdx.x; i < BT_NB * BT_NB; i += 256) out[i] = T[i];
+}
+
+// Z (row-major real) -> X (column-major complex), grid-stride over all batch entries.
+__global__ void k_z_to_x(const double* __restrict__ Z, cplx* __restrict__ X, int n, size_t total) {
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t nn = (size_t)n * n;
+        const size_t mat = idx / nn, rem = idx % nn;
+        const int c = (int)(rem / n), r = (int)(rem % n);
+        X[idx] = mk(Z[mat * nn + (size_t)r * n + c], 0.0);
+    }
+}
+
+// W' = T (V^H X) for block j and 32 columns of X: grid (ceil(n/32), matrices).
+// Thread t owns W rows k0, k0+1 (k0 = 2*(t/8)) and columns c0..c0+3 (c0 = 4*(t%8)).
+__global__ void __launch_bounds__(256)
+k_bt_w(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const cplx* __restrict__ X,
+       cplx* __restrict__ Wp, int n, int j) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    typedef cplx VRow[BT_NB + 1];
+    typedef cplx CRow[33];
+    VRow* Vs = reinterpret_cast<VRow*>(smem_raw);          // [32][65]
+    CRow* Xs = reinterpret_cast<CRow*>(Vs + 32);           // [32][33]
+    CRow* Ws = Xs + 32;                                    // [64][33]
+    const int t = threadIdx.x;
+    const int k0 = 2 * (t / 8), c0 = 4 * (t % 8);
+    const size_t mat = blockIdx.y;
+    const int col0 = blockIdx.x * 32;
+    const cplx* a = A + mat * (size_t)n * n;
+    const cplx* x = X + mat * (size_t)n * n;
+    const int i0 = j * BT_NB, i1 = min(i0 + BT_NB - 1, n - 2);
+    cplx acc[2][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = mk(0, 0);
+    for (int r0 = 0; r0 <= i1; r0 += 32) {
+        __syncthreads();
+        for (int idx = t; idx < 32 * BT_NB; idx += 256) {
+            const int rr = idx / BT_NB, k = idx % BT_NB;
+            Vs[rr][k] = r0 + rr <= i1 ? refl_entry(a, n, i0 + k, r0 + rr) : mk(0, 0);
+        }
+        for (int idx = t; idx < 32 * 32; idx += 256) {
+            const int cc = idx / 32, rr = idx % 32;   // coalesced along rows of column col0+cc
+            Xs[rr][cc] = (r0 + rr <= i1 && col0 + cc < n) ? x[(size_t)(col0 + cc) * n + r0 + rr] : mk(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int rr = 0; rr < 32; ++rr) {
+            const cplx va = Vs[rr][k0], vb = Vs[rr][k0 + 1];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const cplx xv = Xs[rr][c0 + v];
+                cfmac(acc[0][v], va, xv);
+                cfmac(acc[1][v], vb, xv);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) Ws[k0 + u][c0 + v] = acc[u][v];
+    __syncthreads();
+    const int nblk = (n - 1 + BT_NB - 1) / BT_NB;
+    const cplx* T = Tw + (mat * nblk + j) * BT_NB * BT_NB;
+    cplx* wp = Wp + mat * (size_t)BT_NB * n;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const int k = k0 + u;
+        cplx s[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
+        for (int q = 0; q <= k; ++q) {
+            const cplx tq = T[k * BT_NB + q];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) cfma(s[v], tq, Ws[q][c0 + v]);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            if (col0 + c0 + v < n) wp[(size_t)k * n + col0 + c0 + v] = s[v];
+    }
+}
+
+// X[0..i1][cols] -= V W' for block j: grid (row tiles of 64, column tiles of 32, matrices).
+// Thread t owns rows r0+2*(t/8)+{0,1} and columns c0..c0+3.
+__global__ void __launch_bounds__(256)
+k_bt_upd(const cplx* __restrict__ A, const cplx* __restrict__ Wp, cplx* __restrict__ X, int n, int j) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    typedef cplx VRow[BT_NB + 1];
+    typedef cplx CRow[33];
+    VRow* Vs = reinterpret_cast<VRow*>(smem_raw);          // [64][65]
+    CRow* Ws = reinterpret_cast<CRow*>(Vs + 64);           // [64][33]
+    const int t = threadIdx.x;
+    const size_t mat = blockIdx.z;
+    const int row0 = blockIdx.x * 64, col0 = blockIdx.y * 32;
+    const int i0 = j * BT_NB, i1 = min(i0 + BT_NB - 1, n - 2);
+    if (row0 > i1) return;
+    const cplx* a = A + mat * (size_t)n * n;
+    const cplx* wp = Wp + mat * (size_t)BT_NB * n;
+    for (int idx = t; idx < 64 * BT_NB; idx += 256) {
+        const int rr = idx / BT_NB, k = idx % BT_NB;
+        Vs[rr][k] = row0 + rr <= i1 ? refl_entry(a, n, i0 + k, row0 + rr) : mk(0, 0);
+    }
+    for (int idx = t; idx < BT_NB * 32; idx += 256) {
+        const int k = idx / 32, cc = idx % 32;
+        Ws[k][cc] = col0 + cc < n ? wp[(size_t)k * n + col0 + cc] : mk(0, 0);
+    }
+    __syncthreads();
+    const int rl = 2 * (t / 8), c0 = 4 * (t % 8);
+    cplx s[2][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) s[u][v] = mk(0, 0);
+#pragma unroll 4
+    for (int k = 0; k < BT_NB; ++k) {
+        const cplx va = Vs[rl][k], vb = Vs[rl + 1][k];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const cplx w = Ws[k][c0 + v];
+            cfma(s[0][v], va, w);
+            cfma(s[1][v], vb, w);
+        }
+    }
+    cplx* x = X + mat * (size_t)n * n;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const int r = row0 + rl + u;
+        if (r > i1) continue;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int c = col0 + c0 + v;
+            if (c < n) {
+                cplx* p = &x[(size_t)c * n + r];
+                *p = csub(*p, s[u][v]);
+            }
+        }
+    }
+}
+
 // Launch shape of k_hetrd: small matrices keep their whole triangle in shared memory with
 // 128 threads and several CTAs per SM; larger ones run 512 threads, one CTA per SM, with
 // as much of the leading triangle resident as ~220 KB allows.
@@ -974,55 +1170,148 @@ static cudaError_t launch_hetrd(const HetrdCfg& c, cudaStream_t st, int nb, cplx
     return cudaGetLastError();
 }
 
-// Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch.
-size_t heev_scratch_bytes_per_matrix(int n) {
-    const size_t nn = (size_t)n * n;
-    const size_t tblk = (size_t)((n - 1 + ORM_NB - 1) / ORM_NB) * ORM_NB * ORM_NB;
-    return ((size_t)(4 * n) + 8 * nn + 2 * tblk) * sizeof(double);
-}
+// Shape of one eigensolve chunk: kernel configurations and the scratch layout per matrix.
+struct HeevPlan {
+    int n;
+    HetrdCfg hc;
+    size_t smem_tri;
+    bool small_bt;       // k_ormtr (register-resident Z chunk) or the large-order GEMM path
+    int ch, dbuf;
+    size_t smem_orm;
+    int nblk16, nblk64;
+    // per-matrix scratch, in doubles
+    size_t off_d, off_e, off_tau, off_z, off_lu, off_x, off_t, off_w, per;
+};
 
-// The kernel sequence of rlmb_heevd_batched for nb matrices of order n on caller-provided
-// scratch of nb * heev_scratch_bytes_per_matrix(n) bytes (no allocation).  Every scratch
-// region is written by a kernel before any kernel reads it.
-int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n, int nb,
-                          void* scratch, long long* launches) {
-    const size_t nn = (size_t)n * n;
-    const size_t tblk = (size_t)((n - 1 + ORM_NB - 1) / ORM_NB) * ORM_NB * ORM_NB;
-    double* Dw = static_cast<double*>(scratch);
-    double* Ew = Dw + (size_t)nb * n;
-    cplx* TAUw = reinterpret_cast<cplx*>(Ew + (size_t)nb * n);
-    double* Zw = reinterpret_cast<double*>(TAUw + (size_t)nb * n);
-    double* LUw = Zw + (size_t)nb * nn;
-    cplx* Xw = reinterpret_cast<cplx*>(LUw + 5 * (size_t)nb * nn);
-    cplx* Tw = Xw + (size_t)nb * nn;
-    (void)tblk;
-    const HetrdCfg hc = hetrd_config(n);
-    const size_t smem_trd = hc.smem;
-    const size_t smem_tri = 4 * n * sizeof(double) + n * sizeof(int);
+static HeevPlan heev_plan(int n) {
+    HeevPlan p{};
+    p.n = n;
+    p.hc = hetrd_config(n);
+    p.smem_tri = 4 * (size_t)n * sizeof(double) + n * sizeof(int);
+    p.nblk16 = (n - 1 + ORM_NB - 1) / ORM_NB;
+    p.nblk64 = (n - 1 + BT_NB - 1) / BT_NB;
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
-    if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;
-    size_t smem_orm = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
-    const int dbuf = smem_orm <= 220 * 1024 ? 1 : 0;   // double-buffered V blocks when they fit
-    if (!dbuf)
-        smem_orm = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
-                   sizeof(cplx);
-    if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
-    auto ormtr = ch == 16 ? k_ormtr<16> : ch == 8 ? k_ormtr<8> : ch == 4 ? k_ormtr<4> : ch == 2 ? k_ormtr<2> : k_ormtr<1>;
-    if (cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri) != cudaSuccess ||
-        cudaFuncSetAttribute(k_tridiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri) != cudaSuccess ||
-        cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_orm) != cudaSuccess)
+    p.ch = ch;
+    size_t smem = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+    p.dbuf = smem <= 220 * 1024 ? 1 : 0;
+    if (!p.dbuf)
+        smem = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+    p.smem_orm = smem;
+    p.small_bt = (n + 256 / ch - 1) / (256 / ch) <= ORM_RPT && smem <= 220 * 1024;
+    // every region is a multiple of 32 doubles per matrix, so that each region of a chunk
+    // starts 256-byte aligned whatever the chunk size (complex and cp.async accesses)
+    const size_t nn = (size_t)n * n;
+    auto r32 = [](size_t v) { return (v + 31) / 32 * 32; };
+    size_t off = 0;
+    p.off_d = off; off += r32(n);
+    p.off_e = off; off += r32(n);
+    p.off_tau = off; off += r32(2 * (size_t)n);
+    p.off_z = off; off += r32(nn);
+    p.off_lu = off; off += r32(5 * (size_t)n * TRI_THREADS);
+    p.off_x = off; off += r32(2 * nn);
+    p.off_t = off; off += r32(2 * (size_t)(p.small_bt ? p.nblk16 * ORM_NB * ORM_NB : p.nblk64 * BT_NB * BT_NB));
+    p.off_w = off; off += p.small_bt ? 0 : r32(2 * (size_t)BT_NB * n);
+    p.per = off;
+    return p;
+}
+
+// Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch.
+size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n).per * sizeof(double); }
+
+#define RLMB_CHUNK_LAUNCHED()                                     \
+    do {                                                          \
+        if (ctx) {                                                \
+            prof_end(ctx);                                        \
+            ctx->launches++;                                      \
+        } else {                                                  \
+            ++*launches;                                          \
+        }                                                         \
+        if (cudaGetLastError() != cudaSuccess) return RLMB_ERR_CUDA; \
+    } while (0)
+#define RLMB_CHUNK_PROF(name) \
+    do {                      \
+        if (ctx) prof_begin(ctx, name); \
+    } while (0)
+
+// The kernel sequence of one eigensolve chunk of nb matrices of order n on scratch laid out
+// per matrix as heev_plan describes (nb * heev_scratch_bytes_per_matrix(n) bytes, no
+// allocation).  Every scratch region is written by a kernel before any kernel reads it.
+// ctx (optional) receives the launch count and profile; otherwise *launches is advanced.
+static int heev_chunk(rlmb_context* ctx, cudaStream_t st, cplx* A, double* W, int* info, int n, int nb,
+                      void* scratch, long long* launches) {
+    const HeevPlan p = heev_plan(n);
+    double* base = static_cast<double*>(scratch);
+    const size_t B = (size_t)nb;
+    double* Dw = base + p.off_d * B;
+    double* Ew = base + p.off_e * B;
+    cplx* TAUw = reinterpret_cast<cplx*>(base + p.off_tau * B);
+    double* Zw = base + p.off_z * B;
+    double* LUw = base + p.off_lu * B;
+    cplx* Xw = reinterpret_cast<cplx*>(base + p.off_x * B);
+    cplx* Tw = reinterpret_cast<cplx*>(base + p.off_t * B);
+    cplx* Wp = reinterpret_cast<cplx*>(base + p.off_w * B);
+    const size_t nn = (size_t)n * n;
+    if (p.hc.smem > 227 * 1024 || p.smem_tri > 227 * 1024) return RLMB_ERR_ARG;
+    if (cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_tri) != cudaSuccess ||
+        cudaFuncSetAttribute(k_tridiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_tri) != cudaSuccess)
         return RLMB_ERR_CUDA;
-    if (launch_hetrd(hc, st, nb, A, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
-    k_tridiag<1><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
-    k_tridiag<2><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
-    if (n > 1) k_larft<<<nb, 256, 0, st>>>(A, TAUw, Tw, n);
-    ormtr<<<dim3((n + ch - 1) / ch, nb), 256, smem_orm, st>>>(A, Tw, Zw, Xw, n, dbuf);
-    *launches += n > 1 ? 5 : 4;
-    if (cudaGetLastError() != cudaSuccess) return RLMB_ERR_CUDA;
-    if (cudaMemcpyAsync(A, Xw, nb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    RLMB_CHUNK_PROF("k_hetrd");
+    if (launch_hetrd(p.hc, st, nb, A, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_stebz");
+    k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_stein");
+    k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+    RLMB_CHUNK_LAUNCHED();
+    if (p.small_bt) {
+        auto ormtr = p.ch == 16 ? k_ormtr<16> : p.ch == 8 ? k_ormtr<8> : p.ch == 4 ? k_ormtr<4>
+                   : p.ch == 2 ? k_ormtr<2> : k_ormtr<1>;
+        if (cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_orm) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        if (n > 1) {
+            RLMB_CHUNK_PROF("k_larft");
+            k_larft<<<nb, 256, 0, st>>>(A, TAUw, Tw, n);
+            RLMB_CHUNK_LAUNCHED();
+        }
+        RLMB_CHUNK_PROF("k_ormtr");
+        ormtr<<<dim3((n + p.ch - 1) / p.ch, nb), 256, p.smem_orm, st>>>(A, Tw, Zw, Xw, n, p.dbuf);
+        RLMB_CHUNK_LAUNCHED();
+    } else {
+        const size_t smem_t = 2 * BT_NB * BT_NB * sizeof(cplx);
+        const size_t smem_w = (32 * (BT_NB + 1) + 32 * 33 + BT_NB * 33) * sizeof(cplx);
+        const size_t smem_u = (64 * (BT_NB + 1) + BT_NB * 33) * sizeof(cplx);
+        if (cudaFuncSetAttribute(k_larft64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess ||
+            cudaFuncSetAttribute(k_bt_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w) != cudaSuccess ||
+            cudaFuncSetAttribute(k_bt_upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_u) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        RLMB_CHUNK_PROF("k_larft");
+        k_larft64<<<dim3(p.nblk64, nb), 256, smem_t, st>>>(A, TAUw, Tw, n);
+        RLMB_CHUNK_LAUNCHED();
+        RLMB_CHUNK_PROF("k_ormtr");
+        k_z_to_x<<<2048, 256, 0, st>>>(Zw, Xw, n, B * nn);
+        RLMB_CHUNK_LAUNCHED();
+        for (int j = 0; j < p.nblk64; ++j) {
+            const int i1 = std::min(j * BT_NB + BT_NB - 1, n - 2);
+            RLMB_CHUNK_PROF("k_ormtr");
+            k_bt_w<<<dim3((n + 31) / 32, nb), 256, smem_w, st>>>(A, Tw, Xw, Wp, n, j);
+            RLMB_CHUNK_LAUNCHED();
+            RLMB_CHUNK_PROF("k_ormtr");
+            k_bt_upd<<<dim3(i1 / 64 + 1, (n + 31) / 32, nb), 256, smem_u, st>>>(A, Wp, Xw, n, j);
+            RLMB_CHUNK_LAUNCHED();
+        }
+    }
+    if (cudaMemcpyAsync(A, Xw, B * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return RLMB_ERR_CUDA;
     return RLMB_OK;
+}
+#undef RLMB_CHUNK_LAUNCHED
+#undef RLMB_CHUNK_PROF
+
+int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n, int nb, void* scratch,
+                          long long* launches) {
+    return heev_chunk(nullptr, st, A, W, info, n, nb, scratch, launches);
 }
 
 }  // namespace rlmb
@@ -1034,69 +1323,26 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     if (!ctx || !d_a || !d_w || n <= 0 || batch < 0) return RLMB_ERR_ARG;
     if (batch == 0) return RLMB_OK;
     RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
-    cudaStream_t st = ctx->stream;
+    const size_t per = heev_scratch_bytes_per_matrix(n);
+    // workspace: 8 GB, or for large orders enough for two resident matrices per SM (one
+    // CTA each in k_tridiag), capped at 60 % of the free memory
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = (size_t)8 << 30;
+    }
+    size_t budget = std::max<size_t>((size_t)8 << 30, 2 * 148 * per);
+    budget = std::min<size_t>(budget, free_b / 10 * 6 + ctx->ws_bytes);
+    budget = std::max<size_t>(budget, per);
+    size_t chunk = std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)batch));
+    if (int rc = ensure_workspace(ctx, chunk * per)) return rc;
     const size_t nn = (size_t)n * n;
-    // workspace per matrix: D,E (2n), TAU (2n doubles), Z (nn), LU (5nn), X (2nn)
-    const size_t tblk = (size_t)((n - 1 + ORM_NB - 1) / ORM_NB) * ORM_NB * ORM_NB;   // T factors
-    const size_t per = (size_t)(4 * n) + nn + 5 * nn + 2 * nn + 2 * tblk;
-    // process in chunks bounded by a workspace budget (~8 GB)
-    const size_t budget = (size_t)8 << 30;
-    size_t chunk = budget / (per * sizeof(double));
-    if (chunk < 1) chunk = 1;
-    if (chunk > (size_t)batch) chunk = batch;
-    if (int rc = ensure_workspace(ctx, chunk * per * sizeof(double))) return rc;
-    double* ws = reinterpret_cast<double*>(ctx->ws);
-    double* Dw = ws;
-    double* Ew = Dw + chunk * n;
-    cplx* TAUw = reinterpret_cast<cplx*>(Ew + chunk * n);
-    double* Zw = reinterpret_cast<double*>(TAUw + chunk * n);
-    double* LUw = Zw + chunk * nn;
-    cplx* Xw = reinterpret_cast<cplx*>(LUw + 5 * chunk * nn);
-    cplx* Tw = Xw + chunk * nn;
-
-    const HetrdCfg hc = hetrd_config(n);
-    const size_t smem_trd = hc.smem;
-    const size_t smem_tri = 4 * n * sizeof(double) + n * sizeof(int);
-    // back-transform chunk: CH columns per CTA, 256/CH row groups of <= ORM_RPT rows
-    int ch = 16;
-    while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
-    if ((n + 256 / ch - 1) / (256 / ch) > ORM_RPT) return RLMB_ERR_ARG;   // n > 4096
-    const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
-    size_t smem_orm = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
-    const int dbuf = smem_orm <= 220 * 1024 ? 1 : 0;   // double-buffered V blocks when they fit
-    if (!dbuf)
-        smem_orm = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) *
-                   sizeof(cplx);
-    if (smem_trd > 227 * 1024 || smem_tri > 227 * 1024 || smem_orm > 227 * 1024) return RLMB_ERR_ARG;
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_tridiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
-    auto ormtr = ch == 16 ? k_ormtr<16> : ch == 8 ? k_ormtr<8> : ch == 4 ? k_ormtr<4> : ch == 2 ? k_ormtr<2> : k_ormtr<1>;
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_orm));
-
+    long long unused = 0;
     for (size_t b0 = 0; b0 < (size_t)batch; b0 += chunk) {
         const int nb = (int)std::min(chunk, (size_t)batch - b0);
-        cplx* A = reinterpret_cast<cplx*>(d_a) + b0 * nn;
-        prof_begin(ctx, "k_hetrd");
-        RLMB_CUDA_TRY(launch_hetrd(hc, st, nb, A, Dw, Ew, TAUw, n));
-        RLMB_LAUNCHED(ctx);
-        prof_begin(ctx, "k_stebz");
-        k_tridiag<1><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, d_w + b0 * n, Zw, LUw,
-                                                       d_info ? d_info + b0 : nullptr, n);
-        RLMB_LAUNCHED(ctx);
-        prof_begin(ctx, "k_stein");
-        k_tridiag<2><<<nb, TRI_THREADS, smem_tri, st>>>(Dw, Ew, d_w + b0 * n, Zw, LUw,
-                                                       d_info ? d_info + b0 : nullptr, n);
-        RLMB_LAUNCHED(ctx);
-        if (n > 1) {
-            prof_begin(ctx, "k_larft");
-            k_larft<<<nb, 256, 0, st>>>(A, TAUw, Tw, n);
-            RLMB_LAUNCHED(ctx);
-        }
-        dim3 g((n + ch - 1) / ch, nb);
-        prof_begin(ctx, "k_ormtr");
-        ormtr<<<g, 256, smem_orm, st>>>(A, Tw, Zw, Xw, n, dbuf);
-        RLMB_LAUNCHED(ctx);
-        RLMB_CUDA_TRY(cudaMemcpyAsync(A, Xw, nb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+        if (int rc = heev_chunk(ctx, ctx->stream, reinterpret_cast<cplx*>(d_a) + b0 * nn, d_w + b0 * n,
+                                d_info ? d_info + b0 : nullptr, n, nb, ctx->ws, &unused))
+            return rc;
     }
     return RLMB_OK;
 }

@@ -91,6 +91,23 @@ def test_heevd_random(ctx, n):
         _check_eig(M, w[b], X[b], np.linalg.eigvalsh(M))
 
 
+@pytest.mark.parametrize("n", [700, 800, 1000, 1537])
+def test_heevd_large_orders(ctx, n):
+    """Orders past the register-resident back-transform (n > ~720 runs the blocked
+    64-reflector path).  Norm-wise tolerances grow with n like LAPACK's own bounds."""
+    rng = np.random.default_rng(n)
+    mats = [_hermitian(rng, n) for _ in range(2)]
+    w, X = _run_heevd(ctx, mats)
+    for b, M in enumerate(mats):
+        wref = np.linalg.eigvalsh(M)
+        scale = np.abs(wref).max()
+        assert np.abs(w[b] - wref).max() <= 1e-12 * scale
+        res = np.linalg.norm(M @ X[b] - X[b] * w[b][None, :]) / np.linalg.norm(M)
+        assert res <= 2e-15 * n, res
+        orth = np.linalg.norm(X[b].conj().T @ X[b] - np.eye(n))
+        assert orth <= 2e-14 * n, orth
+
+
 @pytest.mark.parametrize("kind", ["identity", "degenerate", "diagonal", "zero", "blocks", "tridiag_split"])
 @pytest.mark.parametrize("n", [7, 48])
 def test_heevd_structured(ctx, kind, n):
@@ -301,6 +318,22 @@ def test_rlm_finite_size_geometries_match_reference(ctx, n_phi):
     """rlm at the finite-size-scaling sizes (impurity concentration 16, g=16, seed 1, sample 0)."""
     d = golden(f"rlm_n{n_phi}_g16_c1_s1_full.npz")
     e, c = ctx.rlm_mesh_solve(n_phi, 1.0, 16.0, 16, 1, 0, 1)
+    assert ctx.last_failures == 0
+    eref, cref = d["energies"][0], d["chern"][0]
+    assert np.abs(e[0] - eref).max() <= 1e-10 * np.abs(eref).max()
+    assert np.array_equal(np.rint(c[0]), np.rint(cref))
+    assert np.abs(c[0] - cref).max() < 1e-8
+
+
+def test_rlm_large_order_matches_reference(ctx):
+    """rlm at n_phi=3000 (48,000 impurities, g=4, seed 1, sample 0): 25 solves of order 3000."""
+    import os
+    from conftest import GOLDEN
+    name = "rlm_n3000_g4_c1_s1_full.npz"
+    if not os.path.exists(os.path.join(GOLDEN, name)):
+        pytest.skip(f"{name} not generated")
+    d = golden(name)
+    e, c = ctx.rlm_mesh_solve(3000, 1.0, 16.0, 4, 1, 0, 1)
     assert ctx.last_failures == 0
     eref, cref = d["energies"][0], d["chern"][0]
     assert np.abs(e[0] - eref).max() <= 1e-10 * np.abs(eref).max()

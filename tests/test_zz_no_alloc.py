@@ -54,7 +54,7 @@ def _same(wa, Xa, wb, Xb):
     assert np.abs(ov - 1).max() < VEC_TOL
 
 
-@pytest.mark.parametrize("n,batch", [(48, 5), (256, 19)])
+@pytest.mark.parametrize("n,batch", [(48, 5), (256, 19), (900, 3)])
 def test_noalloc_matches_batched_twice(n, batch):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -75,7 +75,7 @@ def test_noalloc_rejects_orders_beyond_its_scratch():
         pytest.skip("no CUDA device")
     import rlmb
     lib = rlmb.lib()
-    n = 722
+    n = 954
     a = torch.zeros((1, n, n), dtype=torch.complex128, device="cuda")
     w = torch.zeros((1, n), dtype=torch.float64, device="cuda")
     rc = lib.rlmb_heevd_batched_noalloc(ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(w.data_ptr()), n, 1,
