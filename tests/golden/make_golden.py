@@ -179,6 +179,14 @@ def full_size(which):
                     "energies", "chern", "chern_raw")
             np.savez_compressed(os.path.join(HERE, f"rlm_n{n_phi}_g16_c1_s1_full.npz"),
                                 **{k: v for k, v in r.items() if k in keep})
+    if which == "n3000":
+        # the large rlm geometry (n_phi = 3000, 48,000 impurities, g=4), sample 0 of seed 1:
+        # 25 reference zheevd calls of order 3000 (tens of minutes on 8 cores)
+        r = rlm_reference(3000, 1.0, 16.0, 4, 1, 1, threads=8)
+        keep = ("n_phi", "qc", "ic", "n_mesh", "n_sample", "seed", "impurity_num", "off_head",
+                "energies", "chern", "chern_raw", "energies_mesh")
+        np.savez_compressed(os.path.join(HERE, "rlm_n3000_g4_c1_s1_full.npz"),
+                            **{k: v for k, v in r.items() if k in keep})
 
 
 def run_program(args, workdir):
@@ -237,7 +245,7 @@ def main():
 
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "--full":
-        for w in sys.argv[2:] or ["hlm", "rlm"]:
+        for w in sys.argv[2:] or ["hlm", "rlm", "n3000"]:
             full_size(w)
     else:
         main()
