@@ -52,6 +52,23 @@ int rlmb_profile_entry(rlmb_context* ctx, int index, char* name, int name_cap, d
  * denominator of the FP64 kernels. */
 int rlmb_probe_fp64_peak(rlmb_context* ctx, double* tflops);
 
+/* Precision mode of the context's eigensolves (rlmb_heevd_batched, rlmb_heevd_host and the
+ * mesh solves); no counterpart in the reference, whose precision is fixed at build time
+ * (-DDP, Makefile).  RLMB_PRECISION_FP64 (default): every stage in double precision.
+ * RLMB_PRECISION_MIXED: Householder reduction and back-transformation in single
+ * precision, tridiagonal solve in double, then double-precision refinement of every
+ * eigenpair from the residual R = H X - X diag(w); results are returned in double with
+ * the same layout.  Other values return RLMB_ERR_ARG. */
+#define RLMB_PRECISION_FP64 0
+#define RLMB_PRECISION_MIXED 1
+int rlmb_set_precision(rlmb_context* ctx, int mode);
+int rlmb_get_precision(const rlmb_context* ctx);
+/* Refinement steps of the mixed mode, 1 or 2 (default 2).  Each step roughly squares the
+ * relative eigenvector error: one step from single precision leaves residual and
+ * orthogonality defects of ~1e-12..1e-7 (growing with n), two reach double-precision
+ * level.  Eigenvalues are within ~1e-11 relative after one step. */
+int rlmb_set_refinement_steps(rlmb_context* ctx, int steps);
+
 /* ------------------------------------------------- (b) Hermitian eigensolver
  * Batched full eigendecomposition, double precision, in place.
  * Replaces: mkl_heevd            diag_wrappers/mkl_diag.cpp:2-9   (host, col-major, 'U')

@@ -142,6 +142,8 @@ int rlmb_create(rlmb_context** out, int device) {
     std::memset(ctx, 0, sizeof(*ctx));
     ctx->device = device;
     ctx->stream = 0;
+    ctx->precision = RLMB_PRECISION_FP64;
+    ctx->refine_steps = 2;
     *out = ctx;
     return RLMB_OK;
 }
@@ -166,6 +168,20 @@ int rlmb_set_stream(rlmb_context* ctx, void* stream) {
 }
 
 long long rlmb_launch_count(const rlmb_context* ctx) { return ctx ? ctx->launches : -1; }
+
+int rlmb_set_precision(rlmb_context* ctx, int mode) {
+    if (!ctx || (mode != RLMB_PRECISION_FP64 && mode != RLMB_PRECISION_MIXED)) return RLMB_ERR_ARG;
+    ctx->precision = mode;
+    return RLMB_OK;
+}
+
+int rlmb_get_precision(const rlmb_context* ctx) { return ctx ? ctx->precision : RLMB_ERR_ARG; }
+
+int rlmb_set_refinement_steps(rlmb_context* ctx, int steps) {
+    if (!ctx || steps < 1 || steps > 2) return RLMB_ERR_ARG;
+    ctx->refine_steps = steps;
+    return RLMB_OK;
+}
 
 const char* rlmb_status_string(int status) {
     switch (status) {

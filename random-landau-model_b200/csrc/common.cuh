@@ -49,6 +49,59 @@ __device__ __forceinline__ cplx warp_sum(cplx v) {
     return v;
 }
 
+// -------------------------------------------- single-precision complex (mixed mode)
+typedef float2 cplxf;
+__host__ __device__ __forceinline__ cplxf cadd(cplxf a, cplxf b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ cplxf csub(cplxf a, cplxf b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ cplxf cmul(cplxf a, cplxf b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ cplxf cmulc(cplxf a, cplxf b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ __forceinline__ cplxf cconj(cplxf a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ cplxf cscale(cplxf a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ void cfma(cplxf& acc, cplxf a, cplxf b) {
+    acc.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x));
+    acc.y = fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y));
+}
+__host__ __device__ __forceinline__ void cfmac(cplxf& acc, cplxf a, cplxf b) {
+    acc.x = fmaf(a.x, b.x, fmaf(a.y, b.y, acc.x));
+    acc.y = fmaf(a.x, b.y, fmaf(-a.y, b.x, acc.y));
+}
+__host__ __device__ __forceinline__ float cabs2(cplxf a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ cplxf shfl_xor(cplxf v, int m) {
+    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    return v;
+}
+__device__ __forceinline__ cplxf warp_sum(cplxf v) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v = cadd(v, shfl_xor(v, m));
+    return v;
+}
+
+// Precision-generic access: Cx<R>::T is the complex type of real type R.
+template <class R> struct Cx;
+template <> struct Cx<double> { typedef double2 T; };
+template <> struct Cx<float> { typedef float2 T; };
+template <class C> __host__ __device__ __forceinline__ C cm(double r, double i);
+template <> __host__ __device__ __forceinline__ double2 cm<double2>(double r, double i) { return make_double2(r, i); }
+template <> __host__ __device__ __forceinline__ float2 cm<float2>(double r, double i) {
+    return make_float2((float)r, (float)i);
+}
+template <class C> __host__ __device__ __forceinline__ C cz() { return cm<C>(0.0, 0.0); }
+__host__ __device__ __forceinline__ double2 to_c64(double2 a) { return a; }
+__host__ __device__ __forceinline__ double2 to_c64(float2 a) { return make_double2(a.x, a.y); }
+template <class C> __host__ __device__ __forceinline__ C from_c64(double2 a);
+template <> __host__ __device__ __forceinline__ double2 from_c64<double2>(double2 a) { return a; }
+template <> __host__ __device__ __forceinline__ float2 from_c64<float2>(double2 a) {
+    return make_float2((float)a.x, (float)a.y);
+}
+
 }  // namespace rlmb
 
 // -------------------------------------------------------------------- context
@@ -70,6 +123,10 @@ struct rlmb_context {
     size_t hlm_tables_bytes;
     // optional per-kernel CUDA-event timing (rlmb_profile_enable)
     void* prof;
+    // RLMB_PRECISION_FP64 or RLMB_PRECISION_MIXED, and the mixed mode's refinement
+    // steps (rlmb_set_precision, rlmb_set_refinement_steps)
+    int precision;
+    int refine_steps;
 };
 
 #define RLMB_CUDA_TRY(expr)                                                       \

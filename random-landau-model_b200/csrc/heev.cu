@@ -18,30 +18,29 @@
 //
 // Every wait is a __syncthreads inside one CTA: no inter-CTA dependencies, no spins.
 #include "common.cuh"
+#include "small_eig.cuh"
 
 #include <cfloat>
 #include <cmath>
 
 namespace rlmb {
 
-static constexpr int ORMTR_COLS = 16;       // Z columns per back-transform CTA
-static constexpr int ORMTR_THREADS = 256;
 
 // --------------------------------------------------------------- block reductions
-template <int NT>
-__device__ __forceinline__ double block_sum(double v, double* red) {
+template <int NT, class R>
+__device__ __forceinline__ R block_sum(R v, R* red) {
     v = warp_sum(v);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     __syncthreads();
     if (lane == 0) red[w] = v;
     __syncthreads();
-    double s = 0.0;
+    R s = 0;
 #pragma unroll
     for (int i = 0; i < NT / 32; ++i) s += red[i];
     return s;
 }
-template <int NT>
-__device__ __forceinline__ cplx block_sum(cplx v, double* red) {
+template <int NT, class C, class R>
+__device__ __forceinline__ C block_sum_c(C v, R* red) {
     v = warp_sum(v);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     __syncthreads();
@@ -50,32 +49,19 @@ __device__ __forceinline__ cplx block_sum(cplx v, double* red) {
         red[2 * w + 1] = v.y;
     }
     __syncthreads();
-    cplx s = mk(0, 0);
+    C s = cz<C>();
 #pragma unroll
-    for (int i = 0; i < NT / 32; ++i) s = cadd(s, mk(red[2 * i], red[2 * i + 1]));
+    for (int i = 0; i < NT / 32; ++i) {
+        s.x += red[2 * i];
+        s.y += red[2 * i + 1];
+    }
     return s;
 }
 
-// Transpose-reduce: lane l holds vals[j] (j < 32, the contribution of row l to column j);
-// on return vals[0] on lane l is the sum over all 32 lanes of vals[l].
-__device__ __forceinline__ cplx transpose_reduce32(cplx (&v)[32]) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int s = 16; s >= 1; s >>= 1) {
-        const bool up = (lane & s) != 0;
-#pragma unroll
-        for (int j = 0; j < s; ++j) {
-            cplx send = up ? v[j] : v[j + s];
-            cplx keep = up ? v[j + s] : v[j];
-            v[j] = cadd(keep, shfl_xor(send, s));
-        }
-    }
-    return v[0];
-}
-
-// As transpose_reduce32 for a 16-column group: lane l (and l^16) receives the sum over
-// all 32 lanes of v[l & 15].
-__device__ __forceinline__ cplx transpose_reduce16(cplx (&v)[16]) {
+// Transpose-reduce for a 16-column group: lane l holds v[j] (the contribution of row l
+// to column j); on return lane l (and l^16) holds the sum over all 32 lanes of v[l & 15].
+template <class C>
+__device__ __forceinline__ C transpose_reduce16(C (&v)[16]) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int j = 0; j < 16; ++j) v[j] = cadd(v[j], shfl_xor(v[j], 16));
@@ -84,8 +70,8 @@ __device__ __forceinline__ cplx transpose_reduce16(cplx (&v)[16]) {
         const bool up = (lane & s) != 0;
 #pragma unroll
         for (int j = 0; j < s; ++j) {
-            cplx send = up ? v[j] : v[j + s];
-            cplx keep = up ? v[j + s] : v[j];
+            C send = up ? v[j] : v[j + s];
+            C keep = up ? v[j + s] : v[j];
             v[j] = cadd(keep, shfl_xor(send, s));
         }
     }
@@ -101,7 +87,8 @@ __device__ __forceinline__ void tile_of(int t, int& R, int& C) {
     R = t - c * (c + 1) / 2;
 }
 
-__device__ __forceinline__ void smem_atomic_add(cplx* p, cplx v) {
+template <class C>
+__device__ __forceinline__ void smem_atomic_add(C* p, C v) {
     atomicAdd(&p->x, v.x);
     atomicAdd(&p->y, v.y);
 }
@@ -109,66 +96,68 @@ __device__ __forceinline__ void smem_atomic_add(cplx* p, cplx v) {
 // ------------------------------------------------------------------ k_hetrd
 // Storage of the active leading block: global column-major (ld = n) while it is large,
 // packed upper triangle in shared memory (column c at c(c+1)/2) once it fits.
+template <class C>
 struct GlobalStore {
-    cplx* a;
+    C* a;
     int n;
-    __device__ __forceinline__ cplx* at(int r, int c) const { return a + (size_t)c * n + r; }
+    __device__ __forceinline__ C* at(int r, int c) const { return a + (size_t)c * n + r; }
 };
+template <class C>
 struct SharedStore {
-    cplx* s;
-    __device__ __forceinline__ cplx* at(int r, int c) const { return s + (c * (c + 1) / 2 + r); }
+    C* s;
+    __device__ __forceinline__ C* at(int r, int c) const { return s + (c * (c + 1) / 2 + r); }
 };
 
 // One pass over the upper triangle of the leading m x m block, 32x32 tiles dealt to
 // warps: applies the rank-2 update A -= v w^H + w v^H of the previous reflector (if upd)
 // and accumulates pn += A' vn for the next one (if acc), reading and writing every
-// stored element once.  All 32 loads of a tile are issued before any of its stores.
-template <int NT, class S>
-__device__ __forceinline__ void fused_pass(S st, int m, const cplx* __restrict__ v,
-                                           const cplx* __restrict__ w, bool upd,
-                                           const cplx* __restrict__ vn, bool acc, cplx* pn) {
+// stored element once.  All loads of a 16-column half tile are issued before its stores.
+template <int NT, class C, class S>
+__device__ __forceinline__ void fused_pass(S st, int m, const C* __restrict__ v,
+                                           const C* __restrict__ w, bool upd,
+                                           const C* __restrict__ vn, bool acc, C* pn) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = NT / 32;
     const int nb = (m + 31) / 32;
     const int nitems = nb * (nb + 1);   // two 16-column halves per 32x32 tile
     for (int it = warp; it < nitems; it += NW) {
-        int R, C;
-        tile_of(it >> 1, R, C);
-        const int c0 = C * 32 + 16 * (it & 1);
+        int R, Cb;
+        tile_of(it >> 1, R, Cb);
+        const int c0 = Cb * 32 + 16 * (it & 1);
         if (c0 >= m) continue;
         const int r = R * 32 + lane;
         const bool rin = r < m;
-        const cplx vr = rin ? v[r] : mk(0, 0);
-        const cplx wr = rin ? w[r] : mk(0, 0);
-        const cplx vnr = rin ? vn[r] : mk(0, 0);
-        cplx rowacc = mk(0, 0);
-        cplx e[16];
+        const C vr = rin ? v[r] : cz<C>();
+        const C wr = rin ? w[r] : cz<C>();
+        const C vnr = rin ? vn[r] : cz<C>();
+        C rowacc = cz<C>();
+        C e[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int cc = c0 + j;
-            e[j] = (rin && cc < m && r <= cc) ? *st.at(r, cc) : mk(0, 0);
+            e[j] = (rin && cc < m && r <= cc) ? *st.at(r, cc) : cz<C>();
         }
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int cc = c0 + j;
             const bool valid = rin && cc < m && r <= cc;
-            cplx x = e[j];
+            C x = e[j];
             if (upd) {
-                const cplx vc = cc < m ? v[cc] : mk(0, 0);
-                const cplx wc = cc < m ? w[cc] : mk(0, 0);
-                cplx u = cmul(vr, cconj(wc));
+                const C vc = cc < m ? v[cc] : cz<C>();
+                const C wc = cc < m ? w[cc] : cz<C>();
+                C u = cmul(vr, cconj(wc));
                 cfma(u, wr, cconj(vc));
                 x = csub(x, u);
-                if (r == cc) x.y = 0.0;
+                if (r == cc) x.y = 0;
                 if (valid) *st.at(r, cc) = x;
             }
             if (acc) {
-                const cplx vnc = cc < m ? vn[cc] : mk(0, 0);
+                const C vnc = cc < m ? vn[cc] : cz<C>();
                 if (!valid) {
-                    e[j] = mk(0, 0);
+                    e[j] = cz<C>();
                 } else if (r == cc) {
                     rowacc = cadd(rowacc, cscale(vnc, x.x));
-                    e[j] = mk(0, 0);
+                    e[j] = cz<C>();
                 } else {
                     cfma(rowacc, x, vnc);
                     e[j] = cmulc(x, vnr);   // column partial: conj(A'[r][cc]) vn[r]
@@ -176,7 +165,7 @@ __device__ __forceinline__ void fused_pass(S st, int m, const cplx* __restrict__
             }
         }
         if (acc) {
-            const cplx cs = transpose_reduce16(e);
+            const C cs = transpose_reduce16(e);
             const int cl = c0 + (lane & 15);
             if (lane < 16 && cl < m) smem_atomic_add(&pn[cl], cs);
             if (rin) smem_atomic_add(&pn[r], rowacc);
@@ -184,53 +173,55 @@ __device__ __forceinline__ void fused_pass(S st, int m, const cplx* __restrict__
     }
 }
 
-// Householder reflector of zlarfg for (alpha, x[0..len-1]) held in col[0..len]
-// (alpha = col[len]); returns beta, tau and the scale applied to x.
-__device__ __forceinline__ void reflector(const cplx alpha, double xnorm2, double& beta, cplx& tau,
-                                          cplx& scal) {
-    if (xnorm2 == 0.0 && alpha.y == 0.0) {
+// Householder reflector of zlarfg for (alpha, x) with ||x||^2 = xnorm2: returns beta, tau
+// and the scale applied to x.
+template <class C, class R>
+__device__ __forceinline__ void reflector(const C alpha, R xnorm2, R& beta, C& tau, C& scal) {
+    if (xnorm2 == 0 && alpha.y == 0) {
         beta = alpha.x;
-        tau = mk(0, 0);
-        scal = mk(1, 0);
+        tau = cz<C>();
+        scal = cm<C>(1, 0);
         return;
     }
-    const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
-    beta = alpha.x >= 0.0 ? -nrm : nrm;
-    tau = mk((beta - alpha.x) / beta, -alpha.y / beta);
-    const cplx den = mk(alpha.x - beta, alpha.y);
-    const double dn = cabs2(den);
-    scal = mk(den.x / dn, -den.y / dn);
+    const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
+    beta = alpha.x >= 0 ? -nrm : nrm;
+    tau = cm<C>((beta - alpha.x) / beta, -alpha.y / beta);
+    const C den = cm<C>(alpha.x - beta, alpha.y);
+    const R dn = cabs2(den);
+    scal = cm<C>(den.x / dn, -den.y / dn);
 }
 
 // Unblocked reduction A = Q T Q^H (zhetd2, uplo='U') with look-ahead: step i's rank-2
 // update and step i-1's matrix-vector product share one pass over the leading block.
-// a: n*n col-major (upper triangle).  On exit column c (c >= 1) rows 0..c-2 hold the
-// reflector of step c-1 (its entry c-1 is 1 and not stored), D/E the tridiagonal and TAU
-// the reflector scalars.  The leading block moves into shared memory once its packed
-// upper triangle fits in `tri_cap` elements.
-template <int NT>
+// a: n*n col-major (upper triangle), real type R (double, or float in the mixed mode).
+// On exit column c (c >= 1) rows 0..c-2 hold the reflector of step c-1 (its entry c-1 is
+// 1 and not stored), D/E the tridiagonal (double) and TAU the reflector scalars.  The
+// leading block moves into shared memory once its packed upper triangle fits in
+// `tri_cap` elements.
+template <int NT, class R>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 4)
-k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
-        cplx* __restrict__ TAU, int n, int tri_cap) {
+k_hetrd(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
+        typename Cx<R>::T* __restrict__ TAU, int n, int tri_cap) {
+    typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* v = reinterpret_cast<cplx*>(smem_raw);   // [n] current reflector
-    cplx* w = v + n;                                // [n] its w vector
-    cplx* vn = w + n;                               // [n] next reflector / column buffer
-    cplx* pn = vn + n;                              // [n] A' vn accumulator
-    double* red = reinterpret_cast<double*>(pn + n);  // [2*warps]
-    cplx* tri = reinterpret_cast<cplx*>(red + 2 * (NT / 32));   // packed triangle
+    C* v = reinterpret_cast<C*>(smem_raw);   // [n] current reflector
+    C* w = v + n;                             // [n] its w vector
+    C* vn = w + n;                            // [n] next reflector / column buffer
+    C* pn = vn + n;                           // [n] A' vn accumulator
+    R* red = reinterpret_cast<R*>(pn + n);    // [2*warps]
+    C* tri = reinterpret_cast<C*>(red + 2 * (NT / 32));   // packed triangle
     const int tid = threadIdx.x;
     const size_t mat = blockIdx.x;
-    GlobalStore gs{A + mat * (size_t)n * n, n};
-    SharedStore ss{tri};
+    GlobalStore<C> gs{A + mat * (size_t)n * n, n};
+    SharedStore<C> ss{tri};
     double* dd = D + mat * n;
     double* ee = E + mat * n;
-    cplx* tt = TAU + mat * n;
+    C* tt = TAU + mat * n;
     if (n == 1) {
         if (tid == 0) {
             dd[0] = gs.at(0, 0)->x;
             ee[0] = 0.0;
-            tt[0] = mk(0, 0);
+            tt[0] = cz<C>();
         }
         return;
     }
@@ -238,45 +229,45 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
     // -- prologue: reflector of step n-2 from column n-1, then p = A v over [0..n-2]^2
     {
         const int i = n - 2;
-        double part = 0.0;
+        R part = 0;
         for (int r = tid; r <= i + 1; r += NT) {
-            const cplx x = *gs.at(r, i + 1);
+            const C x = *gs.at(r, i + 1);
             vn[r] = x;
             if (r < i) part += cabs2(x);
         }
-        const double xn2 = block_sum<NT>(part, red);
-        double beta;
-        cplx tau, scal;
+        const R xn2 = block_sum<NT>(part, red);
+        R beta;
+        C tau, scal;
         reflector(vn[i], xn2, beta, tau, scal);
-        const bool act = !(tau.x == 0.0 && tau.y == 0.0);
+        const bool act = !(tau.x == 0 && tau.y == 0);
         __syncthreads();
         for (int r = tid; r < i; r += NT) {
-            const cplx x = act ? cmul(scal, vn[r]) : vn[r];
+            const C x = act ? cmul(scal, vn[r]) : vn[r];
             v[r] = x;
             *gs.at(r, i + 1) = x;
         }
         for (int r = tid; r < n; r += NT) {
-            w[r] = mk(0, 0);
-            pn[r] = mk(0, 0);
+            w[r] = cz<C>();
+            pn[r] = cz<C>();
         }
         if (tid == 0) {
-            v[i] = mk(1.0, 0.0);
+            v[i] = cm<C>(1, 0);
             dd[n - 1] = vn[n - 1].x;
-            *gs.at(i, i + 1) = mk(beta, 0.0);
+            *gs.at(i, i + 1) = cm<C>(beta, 0);
             ee[i] = beta;
             tt[i] = tau;
         }
         __syncthreads();
         fused_pass<NT>(gs, i + 1, v, w, false, v, act, pn);
         __syncthreads();
-        cplx dpart = mk(0, 0);
+        C dpart = cz<C>();
         for (int r = tid; r <= i; r += NT) {
-            const cplx x = cmul(tau, pn[r]);
+            const C x = cmul(tau, pn[r]);
             pn[r] = x;
             cfmac(dpart, x, v[r]);
         }
-        const cplx xv = block_sum<NT>(dpart, red);
-        const cplx al = cscale(cmul(tau, xv), -0.5);
+        const C xv = block_sum_c<NT>(dpart, red);
+        const C al = cscale(cmul(tau, xv), (R)-0.5);
         for (int r = tid; r <= i; r += NT) w[r] = cadd(pn[r], cmul(al, v[r]));
         __syncthreads();
     }
@@ -291,33 +282,33 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
             __syncthreads();
         }
         // (1) updated column i, rows 0..i
-        double part = 0.0;
-        const cplx wi = w[i], vi = v[i];
+        R part = 0;
+        const C wi = w[i], vi = v[i];
         for (int r = tid; r <= i; r += NT) {
-            cplx x = resident ? *ss.at(r, i) : *gs.at(r, i);
-            cplx u = cmul(v[r], cconj(wi));
+            C x = resident ? *ss.at(r, i) : *gs.at(r, i);
+            C u = cmul(v[r], cconj(wi));
             cfma(u, w[r], cconj(vi));
             x = csub(x, u);
             vn[r] = x;
             if (r < i - 1) part += cabs2(x);
-            pn[r] = mk(0, 0);
+            pn[r] = cz<C>();
         }
-        const double xn2 = block_sum<NT>(part, red);
+        const R xn2 = block_sum<NT>(part, red);
         // (2) reflector of step i-1: alpha = A'[i-1][i], x = A'[0..i-2][i]
-        double beta;
-        cplx tau, scal;
+        R beta;
+        C tau, scal;
         reflector(vn[i - 1], xn2, beta, tau, scal);
-        const bool act = !(tau.x == 0.0 && tau.y == 0.0);
+        const bool act = !(tau.x == 0 && tau.y == 0);
         __syncthreads();
         if (tid == 0) dd[i] = vn[i].x;
         for (int r = tid; r < i - 1; r += NT) {
-            const cplx x = act ? cmul(scal, vn[r]) : vn[r];
+            const C x = act ? cmul(scal, vn[r]) : vn[r];
             vn[r] = x;
             *gs.at(r, i) = x;   // reflector storage stays in global memory
         }
         if (tid == 0) {
-            vn[i - 1] = mk(1.0, 0.0);
-            *gs.at(i - 1, i) = mk(beta, 0.0);
+            vn[i - 1] = cm<C>(1, 0);
+            *gs.at(i - 1, i) = cm<C>(beta, 0);
             ee[i - 1] = beta;
             tt[i - 1] = tau;
         }
@@ -327,28 +318,28 @@ k_hetrd(cplx* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
         else fused_pass<NT>(gs, i, v, w, true, vn, act, pn);
         __syncthreads();
         // (4) w' = tau pn - tau/2 (x^H vn) vn; v <- vn
-        cplx dpart = mk(0, 0);
+        C dpart = cz<C>();
         for (int r = tid; r < i; r += NT) {
-            const cplx x = cmul(tau, pn[r]);
+            const C x = cmul(tau, pn[r]);
             pn[r] = x;
             cfmac(dpart, x, vn[r]);
         }
-        const cplx xv = block_sum<NT>(dpart, red);
-        const cplx al = cscale(cmul(tau, xv), -0.5);
+        const C xv = block_sum_c<NT>(dpart, red);
+        const C al = cscale(cmul(tau, xv), (R)-0.5);
         for (int r = tid; r < i; r += NT) {
-            w[r] = act ? cadd(pn[r], cmul(al, vn[r])) : mk(0, 0);
+            w[r] = act ? cadd(pn[r], cmul(al, vn[r])) : cz<C>();
             v[r] = vn[r];
         }
         __syncthreads();
     }
     // -- step 0's update reaches only A[0][0]
     if (tid == 0) {
-        cplx x = resident ? *ss.at(0, 0) : *gs.at(0, 0);
-        cplx u = cmul(v[0], cconj(w[0]));
+        C x = resident ? *ss.at(0, 0) : *gs.at(0, 0);
+        C u = cmul(v[0], cconj(w[0]));
         cfma(u, w[0], cconj(v[0]));
         dd[0] = x.x - u.x;
         ee[n - 1] = 0.0;
-        tt[n - 1] = mk(0, 0);
+        tt[n - 1] = cz<C>();
     }
 }
 
@@ -743,23 +734,27 @@ static constexpr int ORM_NB = 16;     // reflectors per block
 static constexpr int ORM_RPT = 16;    // rows of the Z chunk held per thread
 static constexpr int ORM_VS = ORM_NB + 1;   // padded shared-memory row stride of a V block
 
-__device__ __forceinline__ cplx refl_entry(const cplx* __restrict__ a, int n, int i, int r) {
+template <class C>
+__device__ __forceinline__ C refl_entry(const C* __restrict__ a, int n, int i, int r) {
     // component r of reflector i (zero for i > n-2 padding)
-    if (i > n - 2 || r > i) return mk(0, 0);
-    if (r == i) return mk(1.0, 0.0);
+    if (i > n - 2 || r > i) return cz<C>();
+    if (r == i) return cm<C>(1, 0);
     return a[(size_t)(i + 1) * n + r];
 }
 
 // T factors of every block of one matrix (one CTA per matrix):
 //   T[k][k] = tau_k,  T[k][q] = -tau_k sum_{l=q}^{k-1} (v_k^H v_l) T[l][q]   (q < k)
+template <class R>
 __global__ void __launch_bounds__(256)
-k_larft(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restrict__ Tw, int n) {
-    __shared__ cplx G[ORM_NB][ORM_NB];
-    __shared__ cplx T[ORM_NB][ORM_NB];
+k_larft(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __restrict__ TAU,
+        typename Cx<R>::T* __restrict__ Tw, int n) {
+    typedef typename Cx<R>::T C;
+    __shared__ C G[ORM_NB][ORM_NB];
+    __shared__ C T[ORM_NB][ORM_NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const size_t mat = blockIdx.x;
-    const cplx* a = A + mat * (size_t)n * n;
-    const cplx* tau = TAU + mat * n;
+    const C* a = A + mat * (size_t)n * n;
+    const C* tau = TAU + mat * n;
     const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
     for (int j = 0; j < nblk; ++j) {
         const int i0 = j * ORM_NB;
@@ -768,7 +763,7 @@ k_larft(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restri
             const int k = pr / ORM_NB, l = pr % ORM_NB;
             if (l >= k) continue;
             const int ik = i0 + k, il = i0 + l;
-            cplx s = mk(0, 0);
+            C s = cz<C>();
             if (ik <= n - 2) {
                 for (int r = lane; r <= il; r += 32) cfmac(s, refl_entry(a, n, ik, r), refl_entry(a, n, il, r));
             }
@@ -779,15 +774,15 @@ k_larft(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restri
         if (warp == 0) {
             for (int k = 0; k < ORM_NB; ++k) {
                 const int ik = i0 + k;
-                const cplx tk = ik <= n - 2 ? tau[ik] : mk(0, 0);
+                const C tk = ik <= n - 2 ? tau[ik] : cz<C>();
                 if (lane < ORM_NB) {
-                    cplx val = mk(0, 0);
+                    C val = cz<C>();
                     if (lane == k) {
                         val = tk;
                     } else if (lane < k) {
-                        cplx s = mk(0, 0);
+                        C s = cz<C>();
                         for (int l = lane; l < k; ++l) cfma(s, G[k][l], T[l][lane]);
-                        val = cscale(cmul(tk, s), -1.0);
+                        val = cscale(cmul(tk, s), (R)-1);
                     }
                     T[k][lane] = val;
                 }
@@ -795,15 +790,20 @@ k_larft(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restri
             }
         }
         __syncthreads();
-        cplx* out = Tw + (mat * nblk + j) * ORM_NB * ORM_NB;
+        C* out = Tw + (mat * nblk + j) * ORM_NB * ORM_NB;
         out[threadIdx.x] = T[threadIdx.x / ORM_NB][threadIdx.x % ORM_NB];
         __syncthreads();
     }
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+// asynchronous global -> shared copy of one complex element (16 or 8 bytes)
+__device__ __forceinline__ void cp_async_elem(double2* smem_dst, const double2* gmem_src) {
     const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(float2* smem_dst, const float2* gmem_src) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem_src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -811,19 +811,20 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // Stage block j of V (rows 0..i1, layout [r][k]) and its T factor into shared memory:
 // stored reflector entries by cp.async, the implicit 1 and the zeros below by plain stores.
-__device__ __forceinline__ void stage_block(const cplx* __restrict__ a, const cplx* __restrict__ tsrc,
-                                            cplx* vsb, cplx* tsb, int n, int j) {
+template <class C>
+__device__ __forceinline__ void stage_block(const C* __restrict__ a, const C* __restrict__ tsrc,
+                                            C* vsb, C* tsb, int n, int j) {
     const int t = threadIdx.x;
     const int i0 = j * ORM_NB;
     const int i1 = min(i0 + ORM_NB - 1, n - 2);
     for (int idx = t; idx < (i1 + 1) * ORM_NB; idx += 256) {
         const int r = idx / ORM_NB, k = idx % ORM_NB;
         const int i = i0 + k;
-        cplx* dst = &vsb[r * ORM_VS + k];
-        if (i <= n - 2 && r < i) cp_async16(dst, &a[(size_t)(i + 1) * n + r]);
-        else *dst = (i <= n - 2 && r == i) ? mk(1.0, 0.0) : mk(0, 0);
+        C* dst = &vsb[r * ORM_VS + k];
+        if (i <= n - 2 && r < i) cp_async_elem(dst, &a[(size_t)(i + 1) * n + r]);
+        else *dst = (i <= n - 2 && r == i) ? cm<C>(1, 0) : cz<C>();
     }
-    cp_async16(&tsb[t], &tsrc[t]);
+    cp_async_elem(&tsb[t], &tsrc[t]);
     cp_async_commit();
 }
 
@@ -831,33 +832,34 @@ __device__ __forceinline__ void stage_block(const cplx* __restrict__ a, const cp
 // the chunk of X (column-major, column = eigenvector).  Thread t owns column t % CH and the
 // rows g + RG*q (g = t / CH, RG = 256/CH, q < ORM_RPT) in registers.  With dbuf the next
 // block's V and T are copied asynchronously while the current block is applied.
-template <int CH>
+template <int CH, class R>
 __global__ void __launch_bounds__(256)
-k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* __restrict__ Z,
-        cplx* __restrict__ X, int n, int dbuf) {
+k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __restrict__ Tw,
+        const double* __restrict__ Z, typename Cx<R>::T* __restrict__ X, int n, int dbuf) {
+    typedef typename Cx<R>::T C;
     constexpr int RG = 256 / CH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* vsbuf[2];
-    vsbuf[0] = reinterpret_cast<cplx*>(smem_raw);                    // [n][ORM_VS]
+    C* vsbuf[2];
+    vsbuf[0] = reinterpret_cast<C*>(smem_raw);                    // [n][ORM_VS]
     vsbuf[1] = dbuf ? vsbuf[0] + (size_t)n * ORM_VS : vsbuf[0];
-    cplx* tsbuf[2];
+    C* tsbuf[2];
     tsbuf[0] = vsbuf[0] + (size_t)(dbuf ? 2 : 1) * n * ORM_VS;       // [ORM_NB][ORM_NB]
     tsbuf[1] = dbuf ? tsbuf[0] + ORM_NB * ORM_NB : tsbuf[0];
-    cplx* wsum = tsbuf[0] + (size_t)(dbuf ? 2 : 1) * ORM_NB * ORM_NB;   // [8][ORM_NB][CH]
-    cplx* w2 = wsum + 8 * ORM_NB * CH;                                // [ORM_NB][CH]
+    C* wsum = tsbuf[0] + (size_t)(dbuf ? 2 : 1) * ORM_NB * ORM_NB;   // [8][ORM_NB][CH]
+    C* w2 = wsum + 8 * ORM_NB * CH;                                // [ORM_NB][CH]
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int c = t % CH, g = t / CH;
     const size_t mat = blockIdx.y;
     const int col = blockIdx.x * CH + c;
-    const cplx* a = A + mat * (size_t)n * n;
+    const C* a = A + mat * (size_t)n * n;
     const double* z = Z + mat * (size_t)n * n;
     const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
-    const cplx* tw = Tw + mat * (size_t)nblk * ORM_NB * ORM_NB;
-    cplx x[ORM_RPT];
+    const C* tw = Tw + mat * (size_t)nblk * ORM_NB * ORM_NB;
+    C x[ORM_RPT];
 #pragma unroll
     for (int q = 0; q < ORM_RPT; ++q) {
         const int r = g + RG * q;
-        x[q] = (r < n && col < n) ? mk(z[(size_t)r * n + col], 0.0) : mk(0, 0);
+        x[q] = (r < n && col < n) ? cm<C>(z[(size_t)r * n + col], 0) : cz<C>();
     }
     if (dbuf && nblk > 0) stage_block(a, tw, vsbuf[0], tsbuf[0], n, 0);
     for (int j = 0; j < nblk; ++j) {
@@ -876,17 +878,17 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
             cp_async_wait<0>();
         }
         __syncthreads();
-        const cplx* vs = vsbuf[j & 1];
-        const cplx* ts = tsbuf[j & 1];
+        const C* vs = vsbuf[j & 1];
+        const C* ts = tsbuf[j & 1];
         // partial W = V^H X over this thread's rows
-        cplx wp[ORM_NB];
+        C wp[ORM_NB];
 #pragma unroll
-        for (int k = 0; k < ORM_NB; ++k) wp[k] = mk(0, 0);
+        for (int k = 0; k < ORM_NB; ++k) wp[k] = cz<C>();
 #pragma unroll
         for (int q = 0; q < ORM_RPT; ++q) {
             const int r = g + RG * q;
             if (r <= i1) {
-                const cplx* vr = vs + r * ORM_VS;
+                const C* vr = vs + r * ORM_VS;
 #pragma unroll
                 for (int k = 0; k < ORM_NB; ++k) cfmac(wp[k], vr[k], x[q]);
             }
@@ -900,7 +902,7 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
 #pragma unroll
             for (int k = 0; k < ORM_NB; ++k) wsum[(warp * ORM_NB + k) * CH + lane] = wp[k];
         __syncthreads();
-        cplx wk = mk(0, 0);
+        C wk = cz<C>();
         if (t < ORM_NB * CH) {
             for (int w8 = 0; w8 < 8; ++w8) wk = cadd(wk, wsum[w8 * ORM_NB * CH + t]);
             wsum[t] = wk;   // W[k][c] at t = k*CH + c (slot of warp 0, already read)
@@ -908,21 +910,21 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
         __syncthreads();
         if (t < ORM_NB * CH) {
             const int k = t / CH, cc = t % CH;
-            cplx s = mk(0, 0);
+            C s = cz<C>();
             for (int q2 = 0; q2 <= k; ++q2) cfma(s, ts[k * ORM_NB + q2], wsum[q2 * CH + cc]);
             w2[t] = s;
         }
         __syncthreads();
         // X -= V W2 on rows <= i1
-        cplx wc[ORM_NB];
+        C wc[ORM_NB];
 #pragma unroll
         for (int k = 0; k < ORM_NB; ++k) wc[k] = w2[k * CH + c];
 #pragma unroll
         for (int q = 0; q < ORM_RPT; ++q) {
             const int r = g + RG * q;
             if (r <= i1) {
-                const cplx* vr = vs + r * ORM_VS;
-                cplx s = mk(0, 0);
+                const C* vr = vs + r * ORM_VS;
+                C s = cz<C>();
 #pragma unroll
                 for (int k = 0; k < ORM_NB; ++k) cfma(s, vr[k], wc[k]);
                 x[q] = csub(x[q], s);
@@ -931,14 +933,14 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
         __syncthreads();
     }
     // write the chunk column-major through shared memory (coalesced along rows)
-    cplx* xs = vsbuf[0];   // [CH][n]
+    C* xs = vsbuf[0];   // [CH][n]
 #pragma unroll
     for (int q = 0; q < ORM_RPT; ++q) {
         const int r = g + RG * q;
         if (r < n) xs[(size_t)c * n + r] = x[q];
     }
     __syncthreads();
-    cplx* xo = X + mat * (size_t)n * n;
+    C* xo = X + mat * (size_t)n * n;
     const int col0 = blockIdx.x * CH;
     for (int idx = t; idx < CH * n; idx += 256) {
         const int cc = idx / n, r = idx % n;
@@ -955,23 +957,26 @@ k_ormtr(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const double* _
 static constexpr int BT_NB = 64;
 
 // T factor of block j (reflectors 64j .. 64j+63) of one matrix; grid (blocks, matrices).
+template <class R>
 __global__ void __launch_bounds__(256)
-k_larft64(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __restrict__ Tw, int n) {
+k_larft64(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __restrict__ TAU,
+          typename Cx<R>::T* __restrict__ Tw, int n) {
+    typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* G = reinterpret_cast<cplx*>(smem_raw);   // [64][64]
-    cplx* T = G + BT_NB * BT_NB;                   // [64][64]
+    C* G = reinterpret_cast<C*>(smem_raw);   // [64][64]
+    C* T = G + BT_NB * BT_NB;                   // [64][64]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = blockIdx.x;
     const size_t mat = blockIdx.y;
-    const cplx* a = A + mat * (size_t)n * n;
-    const cplx* tau = TAU + mat * n;
+    const C* a = A + mat * (size_t)n * n;
+    const C* tau = TAU + mat * n;
     const int nblk = (n - 1 + BT_NB - 1) / BT_NB;
     const int i0 = j * BT_NB;
     for (int pr = warp; pr < BT_NB * BT_NB; pr += 8) {
         const int k = pr / BT_NB, l = pr % BT_NB;
         if (l >= k) continue;
         const int ik = i0 + k, il = i0 + l;
-        cplx s = mk(0, 0);
+        C s = cz<C>();
         if (ik <= n - 2)
             for (int r = lane; r <= il; r += 32) cfmac(s, refl_entry(a, n, ik, r), refl_entry(a, n, il, r));
         s = warp_sum(s);
@@ -980,44 +985,46 @@ k_larft64(const cplx* __restrict__ A, const cplx* __restrict__ TAU, cplx* __rest
     __syncthreads();
     for (int k = 0; k < BT_NB; ++k) {
         const int ik = i0 + k;
-        const cplx tk = ik <= n - 2 ? tau[ik] : mk(0, 0);
+        const C tk = ik <= n - 2 ? tau[ik] : cz<C>();
         if (threadIdx.x < BT_NB) {
             const int q = threadIdx.x;
-            cplx val = mk(0, 0);
+            C val = cz<C>();
             if (q == k) {
                 val = tk;
             } else if (q < k) {
-                cplx s = mk(0, 0);
+                C s = cz<C>();
                 for (int l = q; l < k; ++l) cfma(s, G[k * BT_NB + l], T[l * BT_NB + q]);
-                val = cscale(cmul(tk, s), -1.0);
+                val = cscale(cmul(tk, s), (R)-1);
             }
             T[k * BT_NB + q] = val;
         }
         __syncthreads();
     }
-    cplx* out = Tw + (mat * nblk + j) * BT_NB * BT_NB;
+    C* out = Tw + (mat * nblk + j) * BT_NB * BT_NB;
     for (int i = threadIdx.x; i < BT_NB * BT_NB; i += 256) out[i] = T[i];
 }
 
 // Z (row-major real) -> X (column-major complex), grid-stride over all batch entries.
-__global__ void k_z_to_x(const double* __restrict__ Z, cplx* __restrict__ X, int n, size_t total) {
+template <class C>
+__global__ void k_z_to_x(const double* __restrict__ Z, C* __restrict__ X, int n, size_t total) {
     for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
         const size_t nn = (size_t)n * n;
         const size_t mat = idx / nn, rem = idx % nn;
         const int c = (int)(rem / n), r = (int)(rem % n);
-        X[idx] = mk(Z[mat * nn + (size_t)r * n + c], 0.0);
+        X[idx] = cm<C>(Z[mat * nn + (size_t)r * n + c], 0);
     }
 }
 
 // W' = T (V^H X) for block j and 32 columns of X: grid (ceil(n/32), matrices).
 // Thread t owns W rows k0, k0+1 (k0 = 2*(t/8)) and columns c0..c0+3 (c0 = 4*(t%8)).
+template <class C>
 __global__ void __launch_bounds__(256)
-k_bt_w(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const cplx* __restrict__ X,
-       cplx* __restrict__ Wp, int n, int j) {
+k_bt_w(const C* __restrict__ A, const C* __restrict__ Tw, const C* __restrict__ X,
+       C* __restrict__ Wp, int n, int j) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    typedef cplx VRow[BT_NB + 1];
-    typedef cplx CRow[33];
+    typedef C VRow[BT_NB + 1];
+    typedef C CRow[33];
     VRow* Vs = reinterpret_cast<VRow*>(smem_raw);          // [32][65]
     CRow* Xs = reinterpret_cast<CRow*>(Vs + 32);           // [32][33]
     CRow* Ws = Xs + 32;                                    // [64][33]
@@ -1025,31 +1032,31 @@ k_bt_w(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const cplx* __re
     const int k0 = 2 * (t / 8), c0 = 4 * (t % 8);
     const size_t mat = blockIdx.y;
     const int col0 = blockIdx.x * 32;
-    const cplx* a = A + mat * (size_t)n * n;
-    const cplx* x = X + mat * (size_t)n * n;
+    const C* a = A + mat * (size_t)n * n;
+    const C* x = X + mat * (size_t)n * n;
     const int i0 = j * BT_NB, i1 = min(i0 + BT_NB - 1, n - 2);
-    cplx acc[2][4];
+    C acc[2][4];
 #pragma unroll
     for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = mk(0, 0);
+        for (int v = 0; v < 4; ++v) acc[u][v] = cz<C>();
     for (int r0 = 0; r0 <= i1; r0 += 32) {
         __syncthreads();
         for (int idx = t; idx < 32 * BT_NB; idx += 256) {
             const int rr = idx / BT_NB, k = idx % BT_NB;
-            Vs[rr][k] = r0 + rr <= i1 ? refl_entry(a, n, i0 + k, r0 + rr) : mk(0, 0);
+            Vs[rr][k] = r0 + rr <= i1 ? refl_entry(a, n, i0 + k, r0 + rr) : cz<C>();
         }
         for (int idx = t; idx < 32 * 32; idx += 256) {
             const int cc = idx / 32, rr = idx % 32;   // coalesced along rows of column col0+cc
-            Xs[rr][cc] = (r0 + rr <= i1 && col0 + cc < n) ? x[(size_t)(col0 + cc) * n + r0 + rr] : mk(0, 0);
+            Xs[rr][cc] = (r0 + rr <= i1 && col0 + cc < n) ? x[(size_t)(col0 + cc) * n + r0 + rr] : cz<C>();
         }
         __syncthreads();
 #pragma unroll 4
         for (int rr = 0; rr < 32; ++rr) {
-            const cplx va = Vs[rr][k0], vb = Vs[rr][k0 + 1];
+            const C va = Vs[rr][k0], vb = Vs[rr][k0 + 1];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                const cplx xv = Xs[rr][c0 + v];
+                const C xv = Xs[rr][c0 + v];
                 cfmac(acc[0][v], va, xv);
                 cfmac(acc[1][v], vb, xv);
             }
@@ -1062,14 +1069,14 @@ k_bt_w(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const cplx* __re
         for (int v = 0; v < 4; ++v) Ws[k0 + u][c0 + v] = acc[u][v];
     __syncthreads();
     const int nblk = (n - 1 + BT_NB - 1) / BT_NB;
-    const cplx* T = Tw + (mat * nblk + j) * BT_NB * BT_NB;
-    cplx* wp = Wp + mat * (size_t)BT_NB * n;
+    const C* T = Tw + (mat * nblk + j) * BT_NB * BT_NB;
+    C* wp = Wp + mat * (size_t)BT_NB * n;
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         const int k = k0 + u;
-        cplx s[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
+        C s[4] = {cz<C>(), cz<C>(), cz<C>(), cz<C>()};
         for (int q = 0; q <= k; ++q) {
-            const cplx tq = T[k * BT_NB + q];
+            const C tq = T[k * BT_NB + q];
 #pragma unroll
             for (int v = 0; v < 4; ++v) cfma(s[v], tq, Ws[q][c0 + v]);
         }
@@ -1081,11 +1088,12 @@ k_bt_w(const cplx* __restrict__ A, const cplx* __restrict__ Tw, const cplx* __re
 
 // X[0..i1][cols] -= V W' for block j: grid (row tiles of 64, column tiles of 32, matrices).
 // Thread t owns rows r0+2*(t/8)+{0,1} and columns c0..c0+3.
+template <class C>
 __global__ void __launch_bounds__(256)
-k_bt_upd(const cplx* __restrict__ A, const cplx* __restrict__ Wp, cplx* __restrict__ X, int n, int j) {
+k_bt_upd(const C* __restrict__ A, const C* __restrict__ Wp, C* __restrict__ X, int n, int j) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    typedef cplx VRow[BT_NB + 1];
-    typedef cplx CRow[33];
+    typedef C VRow[BT_NB + 1];
+    typedef C CRow[33];
     VRow* Vs = reinterpret_cast<VRow*>(smem_raw);          // [64][65]
     CRow* Ws = reinterpret_cast<CRow*>(Vs + 64);           // [64][33]
     const int t = threadIdx.x;
@@ -1093,34 +1101,34 @@ k_bt_upd(const cplx* __restrict__ A, const cplx* __restrict__ Wp, cplx* __restri
     const int row0 = blockIdx.x * 64, col0 = blockIdx.y * 32;
     const int i0 = j * BT_NB, i1 = min(i0 + BT_NB - 1, n - 2);
     if (row0 > i1) return;
-    const cplx* a = A + mat * (size_t)n * n;
-    const cplx* wp = Wp + mat * (size_t)BT_NB * n;
+    const C* a = A + mat * (size_t)n * n;
+    const C* wp = Wp + mat * (size_t)BT_NB * n;
     for (int idx = t; idx < 64 * BT_NB; idx += 256) {
         const int rr = idx / BT_NB, k = idx % BT_NB;
-        Vs[rr][k] = row0 + rr <= i1 ? refl_entry(a, n, i0 + k, row0 + rr) : mk(0, 0);
+        Vs[rr][k] = row0 + rr <= i1 ? refl_entry(a, n, i0 + k, row0 + rr) : cz<C>();
     }
     for (int idx = t; idx < BT_NB * 32; idx += 256) {
         const int k = idx / 32, cc = idx % 32;
-        Ws[k][cc] = col0 + cc < n ? wp[(size_t)k * n + col0 + cc] : mk(0, 0);
+        Ws[k][cc] = col0 + cc < n ? wp[(size_t)k * n + col0 + cc] : cz<C>();
     }
     __syncthreads();
     const int rl = 2 * (t / 8), c0 = 4 * (t % 8);
-    cplx s[2][4];
+    C s[2][4];
 #pragma unroll
     for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) s[u][v] = mk(0, 0);
+        for (int v = 0; v < 4; ++v) s[u][v] = cz<C>();
 #pragma unroll 4
     for (int k = 0; k < BT_NB; ++k) {
-        const cplx va = Vs[rl][k], vb = Vs[rl + 1][k];
+        const C va = Vs[rl][k], vb = Vs[rl + 1][k];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const cplx w = Ws[k][c0 + v];
+            const C w = Ws[k][c0 + v];
             cfma(s[0][v], va, w);
             cfma(s[1][v], vb, w);
         }
     }
-    cplx* x = X + mat * (size_t)n * n;
+    C* x = X + mat * (size_t)n * n;
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         const int r = row0 + rl + u;
@@ -1129,11 +1137,452 @@ k_bt_upd(const cplx* __restrict__ A, const cplx* __restrict__ Wp, cplx* __restri
         for (int v = 0; v < 4; ++v) {
             const int c = col0 + c0 + v;
             if (c < n) {
-                cplx* p = &x[(size_t)c * n + r];
+                C* p = &x[(size_t)c * n + r];
                 *p = csub(*p, s[u][v]);
             }
         }
     }
+}
+
+// ------------------------------------------------- mixed mode: FP64 refinement kernels
+// The mixed mode reduces and back-transforms in single precision (k_hetrd<.., float>,
+// k_larft / k_ormtr or the blocked path on float), solves the tridiagonal in double
+// (k_tridiag), then refines the eigenpairs (X, lambda) of H in double, in the manner of
+// Ogita & Aishima (2018, "Iterative refinement for symmetric eigenvalue decomposition"),
+// one or two steps:
+//   R = H X - X diag(lambda)                            k_ref_resid     (double)
+//   E = X^H R,  F_ij = E_ij / (lambda_j - lambda_i)     k_ref_coupling  (double, i != j)
+//   F_jj = (1 - x_j^H x_j) / 2,
+//   lambda_j += Re(x_j^H r_j) / x_j^H x_j               k_ref_diag      (double)
+//   X <- X + X F                                        k_ref_update    (single product,
+//                                                                        double sum)
+// X F is a first-order correction of the size of the current error, so a single-precision
+// product carries it; R, E and the diagonal need double.  Each step roughly squares the
+// relative error of the vectors.
+// Eigenvalues closer than 2^-17 of the spectral radius are not separated by the single
+// precision start: chains of such gaps form clusters (k_ref_clusters).  Inside a cluster
+// of at most RF_KMAX members the vectors are re-resolved by a Rayleigh-Ritz step on the
+// cluster's subspace in double (k_ref_cluster_solve: S = X_C^H H X_C = E_CC + G_CC Lambda,
+// G_CC = X_C^H X_C, S y = mu G y; k_ref_cluster_apply: X_C <- X_C Y, lambda_C <- mu).
+// Larger clusters, and pairs whose gap is within 8 |E_ij| (first-order theory would not
+// hold), are orthogonalised only, F_ij = -(x_i^H x_j)/2, and keep Rayleigh quotients.
+static constexpr int RF_T = 64;    // output tile edge
+static constexpr int RF_K = 16;    // inner-dimension step
+static constexpr int RF_KMAX = 8;  // largest cluster resolved by Rayleigh-Ritz
+static constexpr double RF_CLUSTER = 0x1p-17;   // relative gap below which pairs cluster
+
+// R = H X - X diag(lambda): grid (n/64 row tiles, n/64 column tiles, matrices).  Thread
+// t owns rows 4*(t/16)+{0..3} and columns (t%16) + 16*{0..3} of the tile.  H is read from
+// the upper triangle of A (column-major, 'U'), the diagonal's imaginary part ignored.
+template <class XT>
+__global__ void __launch_bounds__(256)
+k_ref_resid(const cplx* __restrict__ A, const XT* __restrict__ X, const double* __restrict__ W,
+            cplx* __restrict__ Res, int n) {
+    __shared__ cplx Hs[RF_K][RF_T + 1];
+    __shared__ cplx Xs[RF_K][RF_T + 1];
+    const int t = threadIdx.x, tr = t / 16, tc = t % 16;
+    const size_t mat = blockIdx.z;
+    const int r0 = blockIdx.x * RF_T, c0 = blockIdx.y * RF_T;
+    const cplx* a = A + mat * (size_t)n * n;
+    const XT* x = X + mat * (size_t)n * n;
+    cplx acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = mk(0, 0);
+    for (int k0 = 0; k0 < n; k0 += RF_K) {
+        __syncthreads();
+        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
+            // on and above the diagonal: down the column (r fastest)
+            const int kk = idx / RF_T, rr = idx % RF_T;
+            const int r = r0 + rr, k = k0 + kk;
+            if (r >= n || k >= n) {
+                Hs[kk][rr] = mk(0, 0);
+            } else if (r <= k) {
+                cplx h = a[(size_t)k * n + r];
+                if (r == k) h.y = 0.0;
+                Hs[kk][rr] = h;
+            }
+        }
+        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
+            // below the diagonal (disjoint entries): along the row (k fastest)
+            const int rr = idx / RF_K, kk = idx % RF_K;
+            const int r = r0 + rr, k = k0 + kk;
+            if (r < n && k < n && r > k) Hs[kk][rr] = cconj(a[(size_t)r * n + k]);
+        }
+        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
+            const int cc = idx / RF_K, kk = idx % RF_K;
+            const int c = c0 + cc, k = k0 + kk;
+            Xs[kk][cc] = (c < n && k < n) ? to_c64(x[(size_t)c * n + k]) : mk(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < RF_K; ++kk) {
+            cplx hv[4], xv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) hv[u] = Hs[kk][4 * tr + u];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) xv[v] = Xs[kk][tc + 16 * v];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) cfma(acc[u][v], hv[u], xv[v]);
+        }
+    }
+    cplx* res = Res + mat * (size_t)n * n;
+    const double* w = W + mat * n;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int c = c0 + tc + 16 * v;
+        if (c >= n) continue;
+        const double lam = w[c];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = r0 + 4 * tr + u;
+            if (r >= n) continue;
+            const cplx xr = to_c64(x[(size_t)c * n + r]);
+            res[(size_t)c * n + r] = mk(acc[u][v].x - lam * xr.x, acc[u][v].y - lam * xr.y);
+        }
+    }
+}
+
+// Clusters of the ascending eigenvalues of each matrix (one thread per matrix): chains of
+// consecutive gaps <= RF_CLUSTER * spectral radius.  cl[j] = (first index, size).
+__global__ void k_ref_clusters(const double* __restrict__ W, int2* __restrict__ cl, int n, int nmat) {
+    const int mat = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mat >= nmat) return;
+    const double* w = W + (size_t)mat * n;
+    int2* c = cl + (size_t)mat * n;
+    const double tau = RF_CLUSTER * fmax(fabs(w[0]), fabs(w[n - 1]));
+    int a = 0;
+    for (int j = 1; j <= n; ++j) {
+        if (j == n || w[j] - w[j - 1] > tau) {
+            for (int m = a; m < j; ++m) c[m] = make_int2(a, j - a);
+            a = j;
+        }
+    }
+}
+
+// double overlap of two columns (single or double storage)
+template <class XT>
+__device__ __forceinline__ cplx col_dot(const XT* __restrict__ xi, const XT* __restrict__ xj, int n) {
+    cplx g = mk(0, 0);
+    for (int k = 0; k < n; ++k) cfmac(g, to_c64(xi[k]), to_c64(xj[k]));
+    return g;
+}
+
+// F_ij = (X^H R)_ij / (lambda_j - lambda_i) for i != j; zero on the diagonal (set by
+// k_ref_diag) and inside Rayleigh-Ritz clusters; -(x_i^H x_j)/2 inside larger clusters and
+// for pairs too close for a first-order correction.  The products are taken in double:
+// F + F^H must cancel the orthogonality defect (E_ij - conj(E_ji) = (lambda_i - lambda_j)
+// x_i^H x_j).
+template <class XT>
+__global__ void __launch_bounds__(256)
+k_ref_coupling(const XT* __restrict__ X, const cplx* __restrict__ Res, const double* __restrict__ W,
+               const int2* __restrict__ CL, cplxf* __restrict__ F, int n) {
+    __shared__ cplx Xs[RF_K][RF_T + 1];
+    __shared__ cplx Rs[RF_K][RF_T + 1];
+    const int t = threadIdx.x, tr = t / 16, tc = t % 16;
+    const size_t mat = blockIdx.z;
+    const int i0 = blockIdx.x * RF_T, j0 = blockIdx.y * RF_T;
+    const XT* x = X + mat * (size_t)n * n;
+    const cplx* res = Res + mat * (size_t)n * n;
+    cplx acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = mk(0, 0);
+    for (int k0 = 0; k0 < n; k0 += RF_K) {
+        __syncthreads();
+        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
+            const int cc = idx / RF_K, kk = idx % RF_K;
+            const int k = k0 + kk;
+            Xs[kk][cc] = (i0 + cc < n && k < n) ? to_c64(x[(size_t)(i0 + cc) * n + k]) : mk(0, 0);
+            Rs[kk][cc] = (j0 + cc < n && k < n) ? res[(size_t)(j0 + cc) * n + k] : mk(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < RF_K; ++kk) {
+            cplx xv[4], rv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) xv[u] = Xs[kk][4 * tr + u];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) rv[v] = Rs[kk][tc + 16 * v];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) cfmac(acc[u][v], xv[u], rv[v]);
+        }
+    }
+    const double* w = W + mat * n;
+    const int2* cl = CL + mat * n;
+    cplxf* f = F + mat * (size_t)n * n;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int j = j0 + tc + 16 * v;
+        if (j >= n) continue;
+        const double lj = w[j];
+        const int2 cj = cl[j];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + 4 * tr + u;
+            if (i >= n) continue;
+            cplxf val = make_float2(0.f, 0.f);
+            if (i != j) {
+                const double gap = lj - w[i];
+                const bool same = cl[i].x == cj.x;
+                if (same && cj.y <= RF_KMAX) {
+                    val = make_float2(0.f, 0.f);   // resolved by k_ref_cluster_solve
+                } else if (!same && fabs(gap) > 8.0 * sqrt(cabs2(acc[u][v]))) {
+                    const double ig = 1.0 / gap;
+                    val = make_float2((float)(acc[u][v].x * ig), (float)(acc[u][v].y * ig));
+                } else {
+                    const cplx g = col_dot(x + (size_t)i * n, x + (size_t)j * n, n);
+                    val = make_float2((float)(-0.5 * g.x), (float)(-0.5 * g.y));
+                }
+            }
+            f[(size_t)j * n + i] = val;
+        }
+    }
+}
+
+// Rayleigh-Ritz on each cluster of 2..RF_KMAX members (one warp per cluster, found at its
+// first index): G = X_C^H X_C and E = X_C^H R_C by warp sums in double, S = E + G Lambda
+// (Hermitian part), then in one lane G = L L^H, C = L^-1 S L^-H, Jacobi C = V diag(mu) V^H,
+// Y = L^-H V (ascending mu).  Y[j][p] (column j's coefficients) and mu[j] go to YB / MU.
+template <class XT>
+__global__ void k_ref_cluster_solve(const XT* __restrict__ X, const cplx* __restrict__ Res,
+                                    const double* __restrict__ W, const int2* __restrict__ CL,
+                                    cplx* __restrict__ YB, double* __restrict__ MU, int n, int nmat) {
+    const int lane = threadIdx.x & 31;
+    const size_t gw = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (gw >= (size_t)nmat * n) return;
+    const size_t mat = gw / n;
+    const int a = (int)(gw % n);
+    const int2 c = CL[mat * n + a];
+    const int k = c.y;
+    if (c.x != a || k < 2 || k > RF_KMAX) return;
+    const XT* x = X + mat * (size_t)n * n;
+    const cplx* res = Res + mat * (size_t)n * n;
+    const double* w = W + mat * n;
+    cplx G[RF_KMAX * RF_KMAX], S[RF_KMAX * RF_KMAX];   // column-major [p + q*k]
+    for (int p = 0; p < k; ++p)
+        for (int q = 0; q < k; ++q) {
+            const XT* xp = x + (size_t)(a + p) * n;
+            const XT* xq = x + (size_t)(a + q) * n;
+            const cplx* rq = res + (size_t)(a + q) * n;
+            cplx g = mk(0, 0), e = mk(0, 0);
+            for (int r = lane; r < n; r += 32) {
+                const cplx xpr = to_c64(xp[r]);
+                cfmac(g, xpr, to_c64(xq[r]));
+                cfmac(e, xpr, rq[r]);
+            }
+            g = warp_sum(g);
+            e = warp_sum(e);
+            G[p + q * k] = g;
+            S[p + q * k] = mk(e.x + w[a + q] * g.x, e.y + w[a + q] * g.y);
+        }
+    if (lane != 0) return;
+    // Hermitian parts
+    for (int p = 0; p < k; ++p)
+        for (int q = p; q < k; ++q) {
+            const cplx gs = cscale(cadd(G[p + q * k], cconj(G[q + p * k])), 0.5);
+            const cplx ss = cscale(cadd(S[p + q * k], cconj(S[q + p * k])), 0.5);
+            G[p + q * k] = gs;
+            G[q + p * k] = cconj(gs);
+            S[p + q * k] = ss;
+            S[q + p * k] = cconj(ss);
+        }
+    // Cholesky G = L L^H (L lower, stored in G's lower triangle and diagonal)
+    for (int j = 0; j < k; ++j) {
+        double d = G[j + j * k].x;
+        for (int m = 0; m < j; ++m) d -= cabs2(G[j + m * k]);
+        if (!(d > 0.0)) {   // not positive definite: leave the cluster as it is
+            for (int q = 0; q < k; ++q) {
+                cplx* yo = YB + (mat * n + a + q) * RF_KMAX;
+                for (int p = 0; p < k; ++p) yo[p] = mk(p == q ? 1.0 : 0.0, 0.0);
+                MU[mat * n + a + q] = w[a + q];
+            }
+            return;
+        }
+        const double ljj = sqrt(d);
+        G[j + j * k] = mk(ljj, 0.0);
+        for (int i = j + 1; i < k; ++i) {
+            cplx s = G[i + j * k];
+            for (int m = 0; m < j; ++m) s = csub(s, cmul(G[i + m * k], cconj(G[j + m * k])));
+            G[i + j * k] = cscale(s, 1.0 / ljj);
+        }
+    }
+    // T = L^-1 S (columns), then C = L^-1 T^H  (= L^-1 S L^-H, Hermitian)
+    cplx T[RF_KMAX * RF_KMAX];
+    for (int q = 0; q < k; ++q)
+        for (int i = 0; i < k; ++i) {
+            cplx s = S[i + q * k];
+            for (int m = 0; m < i; ++m) s = csub(s, cmul(G[i + m * k], T[m + q * k]));
+            T[i + q * k] = cscale(s, 1.0 / G[i + i * k].x);
+        }
+    for (int q = 0; q < k; ++q)
+        for (int i = 0; i < k; ++i) {
+            cplx s = cconj(T[q + i * k]);
+            for (int m = 0; m < i; ++m) s = csub(s, cmul(G[i + m * k], S[m + q * k]));
+            S[i + q * k] = cscale(s, 1.0 / G[i + i * k].x);   // S now holds C
+        }
+    for (int p = 0; p < k; ++p)
+        for (int q = p + 1; q < k; ++q) {
+            const cplx h = cscale(cadd(S[p + q * k], cconj(S[q + p * k])), 0.5);
+            S[p + q * k] = h;
+            S[q + p * k] = cconj(h);
+        }
+    for (int p = 0; p < k; ++p) S[p + p * k].y = 0.0;
+    for (int i = 0; i < k * k; ++i) T[i] = mk(i % (k + 1) == 0 ? 1.0 : 0.0, 0.0);
+    herm_jacobi(S, T, k);   // T <- V
+    // ascending order
+    int order[RF_KMAX];
+    for (int i = 0; i < k; ++i) order[i] = i;
+    for (int i = 1; i < k; ++i)
+        for (int j = i; j > 0 && S[order[j] * (k + 1)].x < S[order[j - 1] * (k + 1)].x; --j) {
+            const int tmp = order[j];
+            order[j] = order[j - 1];
+            order[j - 1] = tmp;
+        }
+    // Y = L^-H V by back substitution, column by column
+    for (int q = 0; q < k; ++q) {
+        const int col = order[q];
+        cplx y[RF_KMAX];
+        for (int i = k - 1; i >= 0; --i) {
+            cplx s = T[i + col * k];
+            for (int m = i + 1; m < k; ++m) s = csub(s, cmul(cconj(G[m + i * k]), y[m]));
+            y[i] = cscale(s, 1.0 / G[i + i * k].x);
+        }
+        cplx* yo = YB + (mat * n + a + q) * RF_KMAX;
+        for (int p = 0; p < k; ++p) yo[p] = y[p];
+        MU[mat * n + a + q] = S[col * (k + 1)].x;
+    }
+}
+
+// Per eigenvector j (one warp each): G_jj = x_j^H x_j and Re(x_j^H r_j) in double;
+// lambda_j += Re(x_j^H r_j) / G_jj (Rayleigh quotient), F_jj = (1 - G_jj) / 2 -- except
+// for members of Rayleigh-Ritz clusters (F_jj = 0, lambda from k_ref_cluster_apply).
+template <class XT>
+__global__ void k_ref_diag(const XT* __restrict__ X, const cplx* __restrict__ Res, const int2* __restrict__ CL,
+                           double* __restrict__ W, cplxf* __restrict__ F, int n, int nmat) {
+    const int lane = threadIdx.x & 31;
+    const size_t gw = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (gw >= (size_t)nmat * n) return;
+    const size_t mat = gw / n;
+    const int j = (int)(gw % n);
+    const int2 c = CL[gw];
+    cplxf* fjj = F + mat * (size_t)n * n + (size_t)j * n + j;
+    if (c.y >= 2 && c.y <= RF_KMAX) {
+        if (lane == 0) *fjj = make_float2(0.f, 0.f);
+        return;
+    }
+    const XT* x = X + mat * (size_t)n * n + (size_t)j * n;
+    const cplx* r = Res + mat * (size_t)n * n + (size_t)j * n;
+    double g = 0.0, q = 0.0;
+    for (int k = lane; k < n; k += 32) {
+        const cplx xv = to_c64(x[k]), rv = r[k];
+        g += xv.x * xv.x + xv.y * xv.y;
+        q += xv.x * rv.x + xv.y * rv.y;
+    }
+    g = warp_sum(g);
+    q = warp_sum(q);
+    if (lane == 0) {
+        W[mat * n + j] += q / g;
+        *fjj = make_float2((float)(0.5 * (1.0 - g)), 0.f);
+    }
+}
+
+// X_out = X + X F (single-precision product, double sum) into a separate buffer.
+template <class XT>
+__global__ void __launch_bounds__(256)
+k_ref_update(const XT* __restrict__ X, const cplxf* __restrict__ F, cplx* __restrict__ Out, int n) {
+    __shared__ cplxf Xs[RF_K][RF_T + 1];
+    __shared__ cplxf Fs[RF_K][RF_T + 1];
+    const int t = threadIdx.x, tr = t / 16, tc = t % 16;
+    const size_t mat = blockIdx.z;
+    const int r0 = blockIdx.x * RF_T, c0 = blockIdx.y * RF_T;
+    const XT* x = X + mat * (size_t)n * n;
+    const cplxf* f = F + mat * (size_t)n * n;
+    cplxf acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = make_float2(0.f, 0.f);
+    for (int k0 = 0; k0 < n; k0 += RF_K) {
+        __syncthreads();
+        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
+            const int kk = idx / RF_T, rr = idx % RF_T;    // X(r, k): r fastest
+            const int r = r0 + rr, k = k0 + kk;
+            Xs[kk][rr] = (r < n && k < n) ? from_c64<cplxf>(to_c64(x[(size_t)k * n + r])) : make_float2(0.f, 0.f);
+        }
+        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
+            const int cc = idx / RF_K, kk = idx % RF_K;    // F(k, c): k fastest
+            const int c = c0 + cc, k = k0 + kk;
+            Fs[kk][cc] = (c < n && k < n) ? f[(size_t)c * n + k] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < RF_K; ++kk) {
+            cplxf xv[4], fv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) xv[u] = Xs[kk][4 * tr + u];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) fv[v] = Fs[kk][tc + 16 * v];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) cfma(acc[u][v], xv[u], fv[v]);
+        }
+    }
+    cplx* out = Out + mat * (size_t)n * n;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int c = c0 + tc + 16 * v;
+        if (c >= n) continue;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = r0 + 4 * tr + u;
+            if (r >= n) continue;
+            const cplx xr = to_c64(x[(size_t)c * n + r]);
+            out[(size_t)c * n + r] = mk(xr.x + (double)acc[u][v].x, xr.y + (double)acc[u][v].y);
+        }
+    }
+}
+
+// X_C <- X_C Y and lambda_C <- mu for every Rayleigh-Ritz cluster (one warp per cluster,
+// rows dealt to lanes; every row is read before it is written, so in place).
+__global__ void k_ref_cluster_apply(cplx* __restrict__ X, const int2* __restrict__ CL, const cplx* __restrict__ YB,
+                                    const double* __restrict__ MU, double* __restrict__ W, int n, int nmat) {
+    const int lane = threadIdx.x & 31;
+    const size_t gw = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (gw >= (size_t)nmat * n) return;
+    const size_t mat = gw / n;
+    const int a = (int)(gw % n);
+    const int2 c = CL[gw];
+    const int k = c.y;
+    if (c.x != a || k < 2 || k > RF_KMAX) return;
+    cplx y[RF_KMAX * RF_KMAX];   // y[p + q*k]
+    for (int q = 0; q < k; ++q)
+        for (int p = 0; p < k; ++p) y[p + q * k] = YB[(mat * n + a + q) * RF_KMAX + p];
+    cplx* x = X + mat * (size_t)n * n + (size_t)a * n;
+    for (int r = lane; r < n; r += 32) {
+        cplx old[RF_KMAX];
+        for (int p = 0; p < k; ++p) old[p] = x[(size_t)p * n + r];
+        for (int q = 0; q < k; ++q) {
+            cplx s = mk(0, 0);
+            for (int p = 0; p < k; ++p) cfma(s, old[p], y[p + q * k]);
+            x[(size_t)q * n + r] = s;
+        }
+    }
+    if (lane < k) W[mat * n + a + lane] = MU[mat * n + a + lane];
+}
+
+// double -> single copy of the matrices (the single-precision reduction works on the copy;
+// the double input stays for the residual)
+__global__ void k_to_single(const cplx* __restrict__ A, cplxf* __restrict__ B, size_t total) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+        B[i] = from_c64<cplxf>(A[i]);
 }
 
 // Launch shape of k_hetrd: small matrices keep their whole triangle in shared memory with
@@ -1144,80 +1593,93 @@ struct HetrdCfg {
     int tri_cap;
     size_t smem;
 };
+template <class R>
 static HetrdCfg hetrd_config(int n) {
+    const size_t ce = 2 * sizeof(R);   // complex element
     const size_t tri_full = (size_t)n * (n + 1) / 2;
-    const size_t vec128 = 4 * (size_t)n * sizeof(cplx) + 2 * (128 / 32) * sizeof(double);
-    if (vec128 + tri_full * sizeof(cplx) <= 76 * 1024)
-        return {128, (int)tri_full, vec128 + tri_full * sizeof(cplx)};
-    const size_t vec512 = 4 * (size_t)n * sizeof(cplx) + 2 * (512 / 32) * sizeof(double);
+    const size_t vec128 = 4 * (size_t)n * ce + 2 * (128 / 32) * sizeof(R);
+    if (vec128 + tri_full * ce <= 76 * 1024) return {128, (int)tri_full, vec128 + tri_full * ce};
+    const size_t vec512 = 4 * (size_t)n * ce + 2 * (512 / 32) * sizeof(R);
     const size_t budget = 220 * 1024;
-    size_t cap = budget > vec512 ? (budget - vec512) / sizeof(cplx) : 0;
+    size_t cap = budget > vec512 ? (budget - vec512) / ce : 0;
     cap = std::min(cap, tri_full);
-    return {512, (int)cap, vec512 + cap * sizeof(cplx)};
+    return {512, (int)cap, vec512 + cap * ce};
 }
-static cudaError_t launch_hetrd(const HetrdCfg& c, cudaStream_t st, int nb, cplx* A, double* D, double* E,
-                                cplx* TAU, int n) {
+template <class R>
+static cudaError_t launch_hetrd(const HetrdCfg& c, cudaStream_t st, int nb, typename Cx<R>::T* A, double* D,
+                                double* E, typename Cx<R>::T* TAU, int n) {
     if (c.smem > 227 * 1024) return cudaErrorInvalidValue;
     if (c.nt == 128) {
-        cudaError_t e = cudaFuncSetAttribute(k_hetrd<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
+        cudaError_t e = cudaFuncSetAttribute(k_hetrd<128, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
         if (e != cudaSuccess) return e;
-        k_hetrd<128><<<nb, 128, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
+        k_hetrd<128, R><<<nb, 128, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
     } else {
-        cudaError_t e = cudaFuncSetAttribute(k_hetrd<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
+        cudaError_t e = cudaFuncSetAttribute(k_hetrd<512, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
         if (e != cudaSuccess) return e;
-        k_hetrd<512><<<nb, 512, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
+        k_hetrd<512, R><<<nb, 512, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
     }
     return cudaGetLastError();
 }
 
-// Shape of one eigensolve chunk: kernel configurations and the scratch layout per matrix.
+// Shape of one eigensolve chunk: kernel configurations and the scratch layout per matrix
+// (byte offsets, each region a multiple of 256 bytes so that every region of a chunk
+// starts aligned whatever the chunk size).
 struct HeevPlan {
     int n;
+    bool mixed;          // single-precision reduction + double refinement
+    int refine_steps;    // mixed mode: 1 or 2
     HetrdCfg hc;
     size_t smem_tri;
-    bool small_bt;       // k_ormtr (register-resident Z chunk) or the large-order GEMM path
+    bool small_bt;       // k_ormtr (register-resident Z chunk) or the blocked GEMM path
     int ch, dbuf;
     size_t smem_orm;
     int nblk16, nblk64;
-    // per-matrix scratch, in doubles
-    size_t off_d, off_e, off_tau, off_z, off_lu, off_x, off_t, off_w, per;
+    size_t off_d, off_e, off_tau, off_a, off_z, off_lu, off_x, off_t, off_w, off_res, off_x1, off_cl,
+        off_y, off_mu, per;
 };
 
-static HeevPlan heev_plan(int n) {
+static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     HeevPlan p{};
     p.n = n;
-    p.hc = hetrd_config(n);
+    p.mixed = mixed;
+    p.refine_steps = mixed ? refine_steps : 0;
+    const size_t ce = mixed ? sizeof(cplxf) : sizeof(cplx);   // working complex element
+    p.hc = mixed ? hetrd_config<float>(n) : hetrd_config<double>(n);
     p.smem_tri = 4 * (size_t)n * sizeof(double) + n * sizeof(int);
     p.nblk16 = (n - 1 + ORM_NB - 1) / ORM_NB;
     p.nblk64 = (n - 1 + BT_NB - 1) / BT_NB;
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     p.ch = ch;
-    size_t smem = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+    size_t smem = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * ce;
     p.dbuf = smem <= 220 * 1024 ? 1 : 0;
     if (!p.dbuf)
-        smem = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * sizeof(cplx);
+        smem = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * ce;
     p.smem_orm = smem;
     p.small_bt = (n + 256 / ch - 1) / (256 / ch) <= ORM_RPT && smem <= 220 * 1024;
-    // every region is a multiple of 32 doubles per matrix, so that each region of a chunk
-    // starts 256-byte aligned whatever the chunk size (complex and cp.async accesses)
     const size_t nn = (size_t)n * n;
-    auto r32 = [](size_t v) { return (v + 31) / 32 * 32; };
+    auto r256 = [](size_t v) { return (v + 255) / 256 * 256; };
     size_t off = 0;
-    p.off_d = off; off += r32(n);
-    p.off_e = off; off += r32(n);
-    p.off_tau = off; off += r32(2 * (size_t)n);
-    p.off_z = off; off += r32(nn);
-    p.off_lu = off; off += r32(5 * (size_t)n * TRI_THREADS);
-    p.off_x = off; off += r32(2 * nn);
-    p.off_t = off; off += r32(2 * (size_t)(p.small_bt ? p.nblk16 * ORM_NB * ORM_NB : p.nblk64 * BT_NB * BT_NB));
-    p.off_w = off; off += p.small_bt ? 0 : r32(2 * (size_t)BT_NB * n);
+    p.off_d = off; off += r256(n * sizeof(double));
+    p.off_e = off; off += r256(n * sizeof(double));
+    p.off_tau = off; off += r256(n * ce);
+    p.off_a = off; off += mixed ? r256(nn * ce) : 0;        // single-precision copy of H, then F
+    p.off_z = off; off += r256(nn * sizeof(double));
+    p.off_lu = off; off += r256(5 * (size_t)n * TRI_THREADS * sizeof(double));
+    p.off_x = off; off += r256(nn * ce);
+    p.off_t = off; off += r256((p.small_bt ? (size_t)p.nblk16 * ORM_NB * ORM_NB : (size_t)p.nblk64 * BT_NB * BT_NB) * ce);
+    p.off_w = off; off += p.small_bt ? 0 : r256((size_t)BT_NB * n * ce);
+    p.off_res = off; off += mixed ? r256(nn * sizeof(cplx)) : 0;
+    p.off_x1 = off; off += p.refine_steps >= 2 ? r256(nn * sizeof(cplx)) : 0;   // step-1 vectors
+    p.off_cl = off; off += mixed ? r256(n * sizeof(int2)) : 0;
+    p.off_y = off; off += mixed ? r256((size_t)n * RF_KMAX * sizeof(cplx)) : 0;
+    p.off_mu = off; off += mixed ? r256(n * sizeof(double)) : 0;
     p.per = off;
     return p;
 }
 
-// Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch.
-size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n).per * sizeof(double); }
+// Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch (double precision).
+size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n, false).per; }
 
 #define RLMB_CHUNK_LAUNCHED()                                     \
     do {                                                          \
@@ -1234,30 +1696,139 @@ size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n).per * sizeof(d
         if (ctx) prof_begin(ctx, name); \
     } while (0)
 
+// Back-transformation X = Q Z in the working precision R (X column-major, column =
+// eigenvector): k_larft + k_ormtr, or for large orders k_larft64 + k_bt_w / k_bt_upd.
+template <class R>
+static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, int nb,
+                          const typename Cx<R>::T* Aw, const typename Cx<R>::T* TAUw, const double* Zw,
+                          typename Cx<R>::T* Xw, typename Cx<R>::T* Tw, typename Cx<R>::T* Wp,
+                          long long* launches) {
+    typedef typename Cx<R>::T C;
+    const int n = p.n;
+    const size_t nn = (size_t)n * n;
+    if (p.small_bt) {
+        auto ormtr = p.ch == 16 ? k_ormtr<16, R> : p.ch == 8 ? k_ormtr<8, R> : p.ch == 4 ? k_ormtr<4, R>
+                   : p.ch == 2 ? k_ormtr<2, R> : k_ormtr<1, R>;
+        if (cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_orm) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        if (n > 1) {
+            RLMB_CHUNK_PROF("k_larft");
+            k_larft<R><<<nb, 256, 0, st>>>(Aw, TAUw, Tw, n);
+            RLMB_CHUNK_LAUNCHED();
+        }
+        RLMB_CHUNK_PROF("k_ormtr");
+        ormtr<<<dim3((n + p.ch - 1) / p.ch, nb), 256, p.smem_orm, st>>>(Aw, Tw, Zw, Xw, n, p.dbuf);
+        RLMB_CHUNK_LAUNCHED();
+        return RLMB_OK;
+    }
+    const size_t smem_t = 2 * BT_NB * BT_NB * sizeof(C);
+    const size_t smem_w = (32 * (BT_NB + 1) + 32 * 33 + BT_NB * 33) * sizeof(C);
+    const size_t smem_u = (64 * (BT_NB + 1) + BT_NB * 33) * sizeof(C);
+    if (cudaFuncSetAttribute(k_larft64<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess ||
+        cudaFuncSetAttribute(k_bt_w<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w) != cudaSuccess ||
+        cudaFuncSetAttribute(k_bt_upd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_u) != cudaSuccess)
+        return RLMB_ERR_CUDA;
+    RLMB_CHUNK_PROF("k_larft");
+    k_larft64<R><<<dim3(p.nblk64, nb), 256, smem_t, st>>>(Aw, TAUw, Tw, n);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ormtr");
+    k_z_to_x<C><<<2048, 256, 0, st>>>(Zw, Xw, n, (size_t)nb * nn);
+    RLMB_CHUNK_LAUNCHED();
+    for (int j = 0; j < p.nblk64; ++j) {
+        const int i1 = std::min(j * BT_NB + BT_NB - 1, n - 2);
+        RLMB_CHUNK_PROF("k_ormtr");
+        k_bt_w<C><<<dim3((n + 31) / 32, nb), 256, smem_w, st>>>(Aw, Tw, Xw, Wp, n, j);
+        RLMB_CHUNK_LAUNCHED();
+        RLMB_CHUNK_PROF("k_ormtr");
+        k_bt_upd<C><<<dim3(i1 / 64 + 1, (n + 31) / 32, nb), 256, smem_u, st>>>(Aw, Wp, Xw, n, j);
+        RLMB_CHUNK_LAUNCHED();
+    }
+    return RLMB_OK;
+}
+
+// One refinement step from the vectors X (single or double) to Out (double, not X).
+template <class XT>
+static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const cplx* A, const XT* X,
+                       double* W, cplx* Res, cplxf* F, int2* CL, cplx* YB, double* MU, cplx* Out,
+                       long long* launches) {
+    const dim3 g((n + RF_T - 1) / RF_T, (n + RF_T - 1) / RF_T, nb);
+    const unsigned gw = (unsigned)(((size_t)nb * n + 7) / 8);   // one warp per column
+    RLMB_CHUNK_PROF("k_ref_resid");
+    k_ref_resid<XT><<<g, 256, 0, st>>>(A, X, W, Res, n);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_clusters");
+    k_ref_clusters<<<(nb + 127) / 128, 128, 0, st>>>(W, CL, n, nb);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_coupling");
+    k_ref_coupling<XT><<<g, 256, 0, st>>>(X, Res, W, CL, F, n);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_cluster");
+    k_ref_cluster_solve<XT><<<gw, 256, 0, st>>>(X, Res, W, CL, YB, MU, n, nb);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_diag");
+    k_ref_diag<XT><<<gw, 256, 0, st>>>(X, Res, CL, W, F, n, nb);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_update");
+    k_ref_update<XT><<<g, 256, 0, st>>>(X, F, Out, n);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_cluster");
+    k_ref_cluster_apply<<<gw, 256, 0, st>>>(Out, CL, YB, MU, W, n, nb);
+    RLMB_CHUNK_LAUNCHED();
+    return RLMB_OK;
+}
+
 // The kernel sequence of one eigensolve chunk of nb matrices of order n on scratch laid out
-// per matrix as heev_plan describes (nb * heev_scratch_bytes_per_matrix(n) bytes, no
-// allocation).  Every scratch region is written by a kernel before any kernel reads it.
-// ctx (optional) receives the launch count and profile; otherwise *launches is advanced.
-static int heev_chunk(rlmb_context* ctx, cudaStream_t st, cplx* A, double* W, int* info, int n, int nb,
-                      void* scratch, long long* launches) {
-    const HeevPlan p = heev_plan(n);
-    double* base = static_cast<double*>(scratch);
+// per matrix as heev_plan describes (nb * plan.per bytes, no allocation).  Every scratch
+// region is written by a kernel before any kernel reads it.  ctx (optional) receives the
+// launch count and profile; otherwise *launches is advanced.
+static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cplx* A, double* W, int* info,
+                      int nb, void* scratch, long long* launches) {
+    const int n = p.n;
+    unsigned char* base = static_cast<unsigned char*>(scratch);
     const size_t B = (size_t)nb;
-    double* Dw = base + p.off_d * B;
-    double* Ew = base + p.off_e * B;
-    cplx* TAUw = reinterpret_cast<cplx*>(base + p.off_tau * B);
-    double* Zw = base + p.off_z * B;
-    double* LUw = base + p.off_lu * B;
-    cplx* Xw = reinterpret_cast<cplx*>(base + p.off_x * B);
-    cplx* Tw = reinterpret_cast<cplx*>(base + p.off_t * B);
-    cplx* Wp = reinterpret_cast<cplx*>(base + p.off_w * B);
+    double* Dw = reinterpret_cast<double*>(base + p.off_d * B);
+    double* Ew = reinterpret_cast<double*>(base + p.off_e * B);
+    double* Zw = reinterpret_cast<double*>(base + p.off_z * B);
+    double* LUw = reinterpret_cast<double*>(base + p.off_lu * B);
     const size_t nn = (size_t)n * n;
     if (p.hc.smem > 227 * 1024 || p.smem_tri > 227 * 1024) return RLMB_ERR_ARG;
     if (cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_tri) != cudaSuccess ||
         cudaFuncSetAttribute(k_tridiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_tri) != cudaSuccess)
         return RLMB_ERR_CUDA;
+    if (!p.mixed) {
+        cplx* TAUw = reinterpret_cast<cplx*>(base + p.off_tau * B);
+        cplx* Xw = reinterpret_cast<cplx*>(base + p.off_x * B);
+        cplx* Tw = reinterpret_cast<cplx*>(base + p.off_t * B);
+        cplx* Wp = reinterpret_cast<cplx*>(base + p.off_w * B);
+        RLMB_CHUNK_PROF("k_hetrd");
+        if (launch_hetrd<double>(p.hc, st, nb, A, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
+        RLMB_CHUNK_LAUNCHED();
+        RLMB_CHUNK_PROF("k_stebz");
+        k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+        RLMB_CHUNK_LAUNCHED();
+        RLMB_CHUNK_PROF("k_stein");
+        k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+        RLMB_CHUNK_LAUNCHED();
+        if (int rc = back_transform<double>(ctx, st, p, nb, A, TAUw, Zw, Xw, Tw, Wp, launches)) return rc;
+        if (cudaMemcpyAsync(A, Xw, B * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        return RLMB_OK;
+    }
+    cplxf* TAUw = reinterpret_cast<cplxf*>(base + p.off_tau * B);
+    cplxf* As = reinterpret_cast<cplxf*>(base + p.off_a * B);
+    cplxf* Xw = reinterpret_cast<cplxf*>(base + p.off_x * B);
+    cplxf* Tw = reinterpret_cast<cplxf*>(base + p.off_t * B);
+    cplxf* Wp = reinterpret_cast<cplxf*>(base + p.off_w * B);
+    cplx* Res = reinterpret_cast<cplx*>(base + p.off_res * B);
+    cplx* X1 = reinterpret_cast<cplx*>(base + p.off_x1 * B);
+    int2* CL = reinterpret_cast<int2*>(base + p.off_cl * B);
+    cplx* YB = reinterpret_cast<cplx*>(base + p.off_y * B);
+    double* MU = reinterpret_cast<double*>(base + p.off_mu * B);
+    RLMB_CHUNK_PROF("k_to_single");
+    k_to_single<<<2048, 256, 0, st>>>(A, As, B * nn);
+    RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_hetrd");
-    if (launch_hetrd(p.hc, st, nb, A, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
+    if (launch_hetrd<float>(p.hc, st, nb, As, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_stebz");
     k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
@@ -1265,45 +1836,15 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, cplx* A, double* W, in
     RLMB_CHUNK_PROF("k_stein");
     k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
     RLMB_CHUNK_LAUNCHED();
-    if (p.small_bt) {
-        auto ormtr = p.ch == 16 ? k_ormtr<16> : p.ch == 8 ? k_ormtr<8> : p.ch == 4 ? k_ormtr<4>
-                   : p.ch == 2 ? k_ormtr<2> : k_ormtr<1>;
-        if (cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_orm) != cudaSuccess)
-            return RLMB_ERR_CUDA;
-        if (n > 1) {
-            RLMB_CHUNK_PROF("k_larft");
-            k_larft<<<nb, 256, 0, st>>>(A, TAUw, Tw, n);
-            RLMB_CHUNK_LAUNCHED();
-        }
-        RLMB_CHUNK_PROF("k_ormtr");
-        ormtr<<<dim3((n + p.ch - 1) / p.ch, nb), 256, p.smem_orm, st>>>(A, Tw, Zw, Xw, n, p.dbuf);
-        RLMB_CHUNK_LAUNCHED();
-    } else {
-        const size_t smem_t = 2 * BT_NB * BT_NB * sizeof(cplx);
-        const size_t smem_w = (32 * (BT_NB + 1) + 32 * 33 + BT_NB * 33) * sizeof(cplx);
-        const size_t smem_u = (64 * (BT_NB + 1) + BT_NB * 33) * sizeof(cplx);
-        if (cudaFuncSetAttribute(k_larft64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess ||
-            cudaFuncSetAttribute(k_bt_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w) != cudaSuccess ||
-            cudaFuncSetAttribute(k_bt_upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_u) != cudaSuccess)
-            return RLMB_ERR_CUDA;
-        RLMB_CHUNK_PROF("k_larft");
-        k_larft64<<<dim3(p.nblk64, nb), 256, smem_t, st>>>(A, TAUw, Tw, n);
-        RLMB_CHUNK_LAUNCHED();
-        RLMB_CHUNK_PROF("k_ormtr");
-        k_z_to_x<<<2048, 256, 0, st>>>(Zw, Xw, n, B * nn);
-        RLMB_CHUNK_LAUNCHED();
-        for (int j = 0; j < p.nblk64; ++j) {
-            const int i1 = std::min(j * BT_NB + BT_NB - 1, n - 2);
-            RLMB_CHUNK_PROF("k_ormtr");
-            k_bt_w<<<dim3((n + 31) / 32, nb), 256, smem_w, st>>>(A, Tw, Xw, Wp, n, j);
-            RLMB_CHUNK_LAUNCHED();
-            RLMB_CHUNK_PROF("k_ormtr");
-            k_bt_upd<<<dim3(i1 / 64 + 1, (n + 31) / 32, nb), 256, smem_u, st>>>(A, Wp, Xw, n, j);
-            RLMB_CHUNK_LAUNCHED();
-        }
-    }
-    if (cudaMemcpyAsync(A, Xw, B * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return RLMB_ERR_CUDA;
+    if (int rc = back_transform<float>(ctx, st, p, nb, As, TAUw, Zw, Xw, Tw, Wp, launches)) return rc;
+    // refinement: the single-precision copy of H is free now and holds F.  Step 1 starts
+    // from the single-precision vectors, step 2 from step 1's double vectors (X1); the
+    // last step writes the caller's buffer (every step's residual reads H first).
+    if (int rc = refine_step<cplxf>(ctx, st, n, nb, A, Xw, W, Res, As, CL, YB, MU,
+                                    p.refine_steps >= 2 ? X1 : A, launches))
+        return rc;
+    if (p.refine_steps >= 2)
+        if (int rc = refine_step<cplx>(ctx, st, n, nb, A, X1, W, Res, As, CL, YB, MU, A, launches)) return rc;
     return RLMB_OK;
 }
 #undef RLMB_CHUNK_LAUNCHED
@@ -1311,7 +1852,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, cplx* A, double* W, in
 
 int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n, int nb, void* scratch,
                           long long* launches) {
-    return heev_chunk(nullptr, st, A, W, info, n, nb, scratch, launches);
+    return heev_chunk(nullptr, st, heev_plan(n, false), A, W, info, nb, scratch, launches);
 }
 
 }  // namespace rlmb
@@ -1323,7 +1864,8 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     if (!ctx || !d_a || !d_w || n <= 0 || batch < 0) return RLMB_ERR_ARG;
     if (batch == 0) return RLMB_OK;
     RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
-    const size_t per = heev_scratch_bytes_per_matrix(n);
+    const HeevPlan plan = heev_plan(n, ctx->precision == RLMB_PRECISION_MIXED, ctx->refine_steps);
+    const size_t per = plan.per;
     // workspace: 8 GB, or for large orders enough for two resident matrices per SM (one
     // CTA each in k_tridiag), capped at 60 % of the free memory
     size_t free_b = 0, total_b = 0;
@@ -1335,13 +1877,14 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     budget = std::min<size_t>(budget, free_b / 10 * 6 + ctx->ws_bytes);
     budget = std::max<size_t>(budget, per);
     size_t chunk = std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)batch));
+    chunk = std::min<size_t>(chunk, 65535);   // grid y / z extent of the per-matrix launches
     if (int rc = ensure_workspace(ctx, chunk * per)) return rc;
     const size_t nn = (size_t)n * n;
     long long unused = 0;
     for (size_t b0 = 0; b0 < (size_t)batch; b0 += chunk) {
         const int nb = (int)std::min(chunk, (size_t)batch - b0);
-        if (int rc = heev_chunk(ctx, ctx->stream, reinterpret_cast<cplx*>(d_a) + b0 * nn, d_w + b0 * n,
-                                d_info ? d_info + b0 : nullptr, n, nb, ctx->ws, &unused))
+        if (int rc = heev_chunk(ctx, ctx->stream, plan, reinterpret_cast<cplx*>(d_a) + b0 * nn, d_w + b0 * n,
+                                d_info ? d_info + b0 : nullptr, nb, ctx->ws, &unused))
             return rc;
     }
     return RLMB_OK;

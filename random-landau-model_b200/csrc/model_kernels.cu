@@ -1,5 +1,6 @@
 // Assembly and Chern-step kernels of the rlm and hlm twist-mesh pipelines (sm_100a, FP64).
 #include "model_kernels.cuh"
+#include "small_eig.cuh"
 
 #include <cfloat>
 #include <cmath>
@@ -324,47 +325,7 @@ __global__ void k_hlm_bloch(int lx, int ly, int Q, int band, int g, int t1_0, in
             else if (r == cc) a[r + cc * Q].y = 0.0;
         }
     for (int i = 0; i < Q * Q; ++i) v[i] = mk(i % (Q + 1) == 0 ? 1.0 : 0.0, 0.0);
-    for (int sweep = 0; sweep < 50; ++sweep) {
-        double off = 0.0, diag = 0.0;
-        for (int cc = 0; cc < Q; ++cc)
-            for (int r = 0; r < Q; ++r) {
-                if (r != cc) off += cabs2(a[r + cc * Q]);
-                else diag += cabs2(a[r + cc * Q]);
-            }
-        if (off <= 1e-32 * fmax(diag, DBL_MIN)) break;
-        for (int p = 0; p < Q - 1; ++p)
-            for (int q = p + 1; q < Q; ++q) {
-                const cplx apq = a[p + q * Q];
-                const double r = sqrt(cabs2(apq));
-                if (r < 1e-300) continue;
-                const cplx e = mk(apq.x / r, apq.y / r);   // apq = r e
-                const double app = a[p + p * Q].x, aqq = a[q + q * Q].x;
-                const double tau = (aqq - app) / (2.0 * r);
-                const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                const double cs = 1.0 / sqrt(1.0 + t * t), sn = t * cs;
-                // G = diag(1, conj(e)) R, R = [[c, s], [-s, c]]; columns p, q of G:
-                // G[:,p] = (c, -s conj(e)), G[:,q] = (s, c conj(e))
-                const cplx gpp = mk(cs, 0.0), gpq = mk(sn, 0.0);
-                const cplx gqp = cscale(cconj(e), -sn), gqq = cscale(cconj(e), cs);
-                for (int k = 0; k < Q; ++k) {   // A <- A G (columns p, q)
-                    const cplx akp = a[k + p * Q], akq = a[k + q * Q];
-                    a[k + p * Q] = cadd(cmul(akp, gpp), cmul(akq, gqp));
-                    a[k + q * Q] = cadd(cmul(akp, gpq), cmul(akq, gqq));
-                    const cplx vkp = v[k + p * Q], vkq = v[k + q * Q];
-                    v[k + p * Q] = cadd(cmul(vkp, gpp), cmul(vkq, gqp));
-                    v[k + q * Q] = cadd(cmul(vkp, gpq), cmul(vkq, gqq));
-                }
-                for (int k = 0; k < Q; ++k) {   // A <- G^H A (rows p, q)
-                    const cplx apk = a[p + k * Q], aqk = a[q + k * Q];
-                    a[p + k * Q] = cadd(cmulc(gpp, apk), cmulc(gqp, aqk));
-                    a[q + k * Q] = cadd(cmulc(gpq, apk), cmulc(gqq, aqk));
-                }
-                a[p + q * Q] = mk(0, 0);
-                a[q + p * Q] = mk(0, 0);
-                a[p + p * Q].y = 0.0;
-                a[q + q * Q].y = 0.0;
-            }
-    }
+    herm_jacobi(a, v, Q);
     // eigenvector of the band-th smallest eigenvalue
     int order[RLMB_MAX_Q];
     for (int i = 0; i < Q; ++i) order[i] = i;

@@ -31,6 +31,9 @@ _SIGNATURES = {
     "rlmb_profile_entry": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
     "rlmb_probe_fp64_peak": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "rlmb_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "rlmb_get_precision": (ctypes.c_int, [_vp]),
+    "rlmb_set_refinement_steps": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rlmb_heevd_batched": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "rlmb_heevd_host": (ctypes.c_int, [_vp, _c_dp, _c_dp, ctypes.c_int, ctypes.c_int]),
     "rlmb_heevd_batched_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
@@ -186,6 +189,21 @@ class Context:
                    "rlmb_profile_entry")
             out[name.value.decode()] = (ms.value, cnt.value)
         return out
+
+    FP64, MIXED = 0, 1
+
+    @property
+    def precision(self):
+        """RLMB_PRECISION_FP64 (0) or RLMB_PRECISION_MIXED (1) for this context's solves."""
+        return lib().rlmb_get_precision(self.h)
+
+    @precision.setter
+    def precision(self, mode):
+        _check(lib().rlmb_set_precision(self.h, int(mode)), "rlmb_set_precision")
+
+    def set_refinement_steps(self, steps):
+        """Mixed mode: 1 or 2 double-precision refinement steps (default 2)."""
+        _check(lib().rlmb_set_refinement_steps(self.h, int(steps)), "rlmb_set_refinement_steps")
 
     def fp64_peak_tflops(self):
         t = ctypes.c_double()

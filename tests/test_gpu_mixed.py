@@ -1,0 +1,211 @@
+"""The mixed-precision mode (RLMB_PRECISION_MIXED: single-precision reduction and
+back-transformation, double tridiagonal solve, double refinement of every eigenpair)
+against the oracle, the reference's golden fixtures and the double-precision mode.
+
+Tolerances (the accuracy contract of the mixed mode with its default two refinement steps):
+  eigenvalues        max|w - w_ref| <= 1e-10 * max|w_ref|
+  residual           ||M X - X diag(w)||_F <= 1e-10 * ||M||_F
+  orthogonality      ||X^H X - I||_F <= 1e-10
+  Chern numbers      rint() identical to the reference, |C - C_ref| <= 1e-8
+  twist energies     max|E - E_ref| <= 1e-10 * max|E_ref|
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+from test_gpu_parity import _hermitian
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+EIG_TOL, RES_TOL, ORTH_TOL = 1e-10, 1e-10, 1e-10
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import rlmb
+    c = rlmb.Context(0)
+    c.precision = c.MIXED
+    assert c.precision == 1
+    yield c
+    c.close()
+
+
+def _solve(ctx, mats):
+    a = torch.tensor(np.stack([m.T for m in mats]), dtype=torch.complex128, device="cuda").contiguous()
+    info = torch.zeros(len(mats), dtype=torch.int32, device="cuda")
+    w = ctx.heevd(a, info=info)
+    torch.cuda.synchronize()
+    assert int(info.abs().sum()) == 0
+    X = a.cpu().numpy()
+    return w.cpu().numpy(), [X[b].T for b in range(len(mats))]
+
+
+def _check(M, w, X, wref):
+    scale = max(np.abs(wref).max(), 1e-300)
+    err = np.abs(np.sort(w) - wref).max() / scale
+    assert err <= EIG_TOL, err
+    nrm = max(np.linalg.norm(M), 1e-300)
+    res = np.linalg.norm(M @ X - X * w[None, :]) / nrm
+    assert res <= RES_TOL, res
+    orth = np.linalg.norm(X.conj().T @ X - np.eye(M.shape[0]))
+    assert orth <= ORTH_TOL, orth
+    return err, res, orth
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 33, 64, 128, 256, 512, 800, 1000])
+def test_mixed_heevd_random(ctx, n):
+    rng = np.random.default_rng(1000 + n)
+    mats = [_hermitian(rng, n) for _ in range(3 if n <= 512 else 2)]
+    w, X = _solve(ctx, mats)
+    for b, M in enumerate(mats):
+        _check(M, w[b], X[b], np.linalg.eigvalsh(M))
+
+
+@pytest.mark.parametrize("kind", ["identity", "degenerate", "diagonal", "zero", "blocks", "tridiag_split"])
+@pytest.mark.parametrize("n", [7, 48])
+def test_mixed_heevd_structured(ctx, kind, n):
+    rng = np.random.default_rng(11 * n)
+    M = _hermitian(rng, n, kind)
+    w, X = _solve(ctx, [M])
+    if kind == "zero":
+        assert np.abs(w[0]).max() == 0.0
+        assert np.linalg.norm(X[0].conj().T @ X[0] - np.eye(n)) <= ORTH_TOL
+        return
+    _check(M, w[0], X[0], np.linalg.eigvalsh(M))
+
+
+@pytest.mark.parametrize("gap", [1e-3, 1e-5, 1e-7, 1e-9, 1e-12, 0.0])
+def test_mixed_close_pairs(ctx, gap):
+    """Uniformly spread eigenvalues (no level repulsion, as for localised states) with one
+    pair `gap` apart relative to the spectral radius 1: pairs the single-precision start
+    cannot separate are re-resolved in double by the cluster Rayleigh-Ritz step."""
+    rng = np.random.default_rng(21)
+    n = 96
+    q = np.linalg.qr(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))[0]
+    w = np.sort(rng.uniform(-1, 1, n))
+    w[0], w[-1] = -1.0, 1.0
+    w[40] = w[39] + gap
+    M = (q * w) @ q.conj().T
+    M = (M + M.conj().T) / 2
+    wm, X = _solve(ctx, [M])
+    _check(M, wm[0], X[0], np.linalg.eigvalsh(M))
+
+
+def test_mixed_reads_upper_triangle_only(ctx):
+    rng = np.random.default_rng(5)
+    M = _hermitian(rng, 40)
+    buf = M.copy()
+    buf[np.tril_indices(40, -1)] = 1e3 + 7j   # garbage below the diagonal, as LAPACK 'U' allows
+    buf[np.diag_indices(40)] += 0.5j          # imaginary diagonal parts are ignored
+    w, X = _solve(ctx, [buf])
+    _check(M, w[0], X[0], np.linalg.eigvalsh(M))
+
+
+def test_mixed_one_step_eigenvalues(ctx):
+    """One refinement step already gives eigenvalues to 1e-10 (the vectors to ~1e-7)."""
+    rng = np.random.default_rng(9)
+    mats = [_hermitian(rng, 300) for _ in range(2)]
+    ctx.set_refinement_steps(1)
+    try:
+        w, X = _solve(ctx, mats)
+    finally:
+        ctx.set_refinement_steps(2)
+    for b, M in enumerate(mats):
+        wref = np.linalg.eigvalsh(M)
+        assert np.abs(w[b] - wref).max() <= EIG_TOL * np.abs(wref).max()
+        assert np.linalg.norm(M @ X[b] - X[b] * w[b][None, :]) <= 1e-6 * np.linalg.norm(M)
+
+
+def test_mixed_matches_double_mode(ctx):
+    """Same matrices through both modes: eigenvalues agree to the double mode's accuracy
+    and eigenvectors up to a phase each."""
+    import rlmb
+    rng = np.random.default_rng(77)
+    mats = [_hermitian(rng, 200) for _ in range(4)]
+    wm, Xm = _solve(ctx, mats)
+    c64 = rlmb.Context(0)
+    wd, Xd = _solve(c64, mats)
+    c64.close()
+    for b in range(len(mats)):
+        assert np.abs(wm[b] - wd[b]).max() <= 1e-11 * np.abs(wd[b]).max()
+        ov = np.abs(np.einsum("rk,rk->k", np.conj(Xm[b]), Xd[b]))
+        assert np.abs(ov - 1).max() < 1e-9
+
+
+def test_precision_mode_arguments(ctx):
+    import rlmb
+    lib = rlmb.lib()
+    assert lib.rlmb_set_precision(ctx.h, 7) == -1
+    assert lib.rlmb_set_refinement_steps(ctx.h, 0) == -1
+    assert lib.rlmb_set_refinement_steps(ctx.h, 3) == -1
+    assert ctx.precision == 1
+
+
+RLM_CASES = ["rlm_n16_g8_c2_s1.npz", "rlm_n64_g4_c1_s3.npz", "rlm_n128_g2_c1_s5.npz", "rlm_n16_g64_c2_s1.npz"]
+
+
+@pytest.mark.parametrize("name", RLM_CASES)
+def test_mixed_rlm_mesh_matches_reference(ctx, name):
+    d = golden(name)
+    ns = int(d["n_sample"])
+    e, c = ctx.rlm_mesh_solve(int(d["n_phi"]), float(d["qc"]), float(d["ic"]), int(d["n_mesh"]),
+                              int(d["seed"]), 0, ns)
+    for s in range(ns):
+        eref, cref = d["energies"][s], d["chern"][s]
+        assert np.abs(e[s] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[s]), np.rint(cref))
+        assert np.abs(c[s] - cref).max() < 1e-8
+
+
+@pytest.mark.parametrize("n_phi", [64, 256, 512])
+def test_mixed_rlm_finite_size_geometries(ctx, n_phi):
+    d = golden(f"rlm_n{n_phi}_g16_c1_s1_full.npz")
+    e, c = ctx.rlm_mesh_solve(n_phi, 1.0, 16.0, 16, 1, 0, 1)
+    eref, cref = d["energies"][0], d["chern"][0]
+    assert np.abs(e[0] - eref).max() <= 1e-10 * np.abs(eref).max()
+    assert np.array_equal(np.rint(c[0]), np.rint(cref))
+    assert np.abs(c[0] - cref).max() < 1e-8
+
+
+@pytest.mark.parametrize("name", ["hlm_3x3_q3_g64_c2_s1.npz", "hlm_9x6_q3_b1_g8_c1_s2.npz",
+                                  "hlm_48x16_q3_b0_g2_c1_s1.npz"])
+def test_mixed_hlm_mesh_matches_reference(ctx, name):
+    d = golden(name)
+    lx, ly, Q, b, g = (int(d[k]) for k in ("lx", "ly", "Q", "band", "n_mesh"))
+    e, c = ctx.hlm_mesh_solve(lx, ly, Q, b, g, d["potentials"])
+    for s in range(int(d["n_sample"])):
+        eref, cref = d["energies"][s], d["chern"][s]
+        assert np.abs(e[s] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[s]), np.rint(cref))
+        assert np.abs(c[s] - cref).max() < 1e-8
+
+
+def test_mixed_hlm_benchmark_geometry(ctx):
+    """The benchmarked hlm geometry (48 x 16, q=3, g=32) on the reference's samples 0, 5, 22."""
+    d = golden("hlm_48x16_q3_b0_g32_s1_full.npz")
+    e, c = ctx.hlm_mesh_solve(48, 16, 3, 0, 32, d["potentials"])
+    for i in range(len(d["samples"])):
+        eref, cref = d["energies"][i], d["chern"][i]
+        assert np.abs(e[i] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[i]), np.rint(cref))
+        assert np.abs(c[i] - cref).max() < 1e-8
+
+
+def test_mixed_rlm_large_order(ctx):
+    """n_phi = 3000, g = 4: the configuration where single precision lost Chern quantisation
+    in the reference's GPU path."""
+    name = "rlm_n3000_g4_c1_s1_full.npz"
+    if not os.path.exists(os.path.join(GOLDEN, name)):
+        pytest.skip(f"{name} not generated")
+    d = golden(name)
+    e, c = ctx.rlm_mesh_solve(3000, 1.0, 16.0, 4, 1, 0, 1)
+    eref, cref = d["energies"][0], d["chern"][0]
+    assert np.abs(e[0] - eref).max() <= 1e-10 * np.abs(eref).max()
+    assert np.array_equal(np.rint(c[0]), np.rint(cref))
+    assert np.abs(c[0] - cref).max() < 1e-8
