@@ -289,6 +289,34 @@ def run_gpu(args):
     barrier()
     ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))
 
+    # ---- the mixed-precision mode on the same inputs (device-resident, same step)
+    mixed = None
+    if not args.no_mixed:
+        c64 = d_c.cpu().numpy()
+        e64 = d_e.cpu().numpy()
+        ctx.precision = ctx.MIXED
+        step_device()
+        barrier()
+        ctx.profile(True)
+        ev0.record()
+        for _ in range(args.steps):
+            step_device()
+        ev1.record()
+        barrier()
+        ms_mix = max_over_ranks(ev0.elapsed_time(ev1))
+        prof_mix = ctx.profile_report()
+        ctx.profile(False)
+        ctx.precision = ctx.FP64
+        cm_, em_ = d_c.cpu().numpy(), d_e.cpu().numpy()
+        v_mix = ws * SOLVES_PER_STEP * args.steps / (ms_mix * 1e-3)
+        mixed = {"value": v_mix, "unit": UNIT, "ms_per_step": ms_mix / args.steps,
+                 "samples_per_hour": v_mix / KPTS * 3600.0,
+                 "refinement_steps": 2,
+                 "chern_integers_identical_to_fp64": bool(np.array_equal(np.rint(cm_), np.rint(c64))),
+                 "max_chern_deviation_from_fp64": float(np.abs(cm_ - c64).max()),
+                 "max_energy_rel_error_vs_fp64": float(np.abs(em_ - e64).max() / np.abs(e64).max()),
+                 "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof_mix.items())}}
+
     value = ws * SOLVES_PER_STEP * args.steps / (ms_dev * 1e-3)
     e2e = ws * SOLVES_PER_STEP * args.steps / (ms_e2e * 1e-3)
     line = None
@@ -310,7 +338,7 @@ def run_gpu(args):
                     "peak_source": "measured in this run: FP64 FMA throughput probe "
                                    "(MEASURED_PEAKS.json holds no FP64 figure)",
                     "share_of_gpu_time": kms / total_ms}
-        eig_ms = sum(prof.get(k, (0, 0))[0] for k in ("k_hetrd", "k_tridiag", "k_ormtr"))
+        eig_ms = sum(prof.get(k, (0, 0))[0] for k in ("k_hetrd", "k_stebz", "k_stein", "k_larft", "k_ormtr"))
         eig_tflops = 13.33 * N_PHI ** 3 * SOLVES_PER_STEP * args.steps / (eig_ms * 1e-3) / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -324,8 +352,10 @@ def run_gpu(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(pots_h.nbytes),
                     "d2h_bytes_per_step": int(2 * NS * N_PHI * 8)},
             "roofline": roof,
-            "eigensolve_roofline": {"flops_per_solve": "13.33 n^3", "achieved_tflops": eig_tflops,
-                                    "peak_tflops": peak, "frac": eig_tflops / peak},
+            "eigensolve_roofline": {"flops_per_solve": "13.33 n^3", "kernels": "hetrd+stebz+stein+larft+ormtr",
+                                    "achieved_tflops": eig_tflops, "peak_tflops": peak,
+                                    "frac": eig_tflops / peak},
+            "mixed": mixed,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
             "gpu_launches": int(launches),
             "clocks": clk,
@@ -338,6 +368,75 @@ def run_gpu(args):
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
+
+
+RLM_WORKLOADS = {
+    # name: (n_phi, g, samples per step) -- rlm with impurity concentration 16, +-1 strengths
+    "rlm512": (512, 16, 32),
+    "rlm3000": (3000, 4, 8),
+}
+
+
+def run_gpu_rlm(args):
+    """rlm workloads (n_phi=512, g=16, 32 samples; n_phi=3000, g=4, 8 samples): one
+    rlmb_rlm_mesh_solve call per step (host disorder generation, device assembly, eigensolve
+    and Chern step, energies and Chern numbers returned to the host), both precisions.
+    Each step solves new samples (sample index advances by the samples per step)."""
+    import numpy as np
+    import torch
+    import rlmb
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    n_phi, g, ns = RLM_WORKLOADS[args.workload]
+    kpts = (g + 1) ** 2
+    ctx = rlmb.Context(local)
+    out = {}
+    for mode in ("fp64", "mixed"):
+        ctx.precision = ctx.MIXED if mode == "mixed" else ctx.FP64
+        sample = 0
+        for _ in range(args.warmup):
+            ctx.rlm_mesh_solve(n_phi, 1.0, 16.0, g, SEED, sample, ns)
+            sample += ns
+        ctx.profile(True)
+        l0 = ctx.launches
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = []
+        for _ in range(args.steps):
+            res.append(ctx.rlm_mesh_solve(n_phi, 1.0, 16.0, g, SEED, sample, ns))
+            sample += ns
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        prof = ctx.profile_report()
+        ctx.profile(False)
+        v = ns * kpts * args.steps / dt
+        out[mode] = {"value": v, "ms_per_step": 1e3 * dt / args.steps, "samples_per_hour": v / kpts * 3600,
+                     "launches": ctx.launches - l0, "results": res,
+                     "kernel_ms_per_step": {k: x[0] / args.steps for k, x in sorted(prof.items())}}
+    c64 = np.concatenate([r[1] for r in out["fp64"]["results"]])
+    cmx = np.concatenate([r[1] for r in out["mixed"]["results"]])
+    e64 = np.concatenate([r[0] for r in out["fp64"]["results"]])
+    emx = np.concatenate([r[0] for r in out["mixed"]["results"]])
+    f, m = out["fp64"], out["mixed"]
+    line = {"metric": METRIC, "value": f["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": f["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"rlm n_phi={n_phi}, impurity concentration 16 (+-1 strengths), "
+                                   f"g={g} ({kpts} k-points/sample), {ns} samples/step, seed {SEED}",
+                       "api": "rlmb_rlm_mesh_solve (host results; disorder drawn on the host)",
+                       "samples_per_hour": f["samples_per_hour"],
+                       "l2": f"each matrix is {16 * n_phi * n_phi / 1e6:.1f} MB; a step's matrices exceed L2"},
+            "kernel_ms_per_step": f["kernel_ms_per_step"], "gpu_launches": f["launches"],
+            "mixed": {"value": m["value"], "ms_per_step": m["ms_per_step"],
+                      "samples_per_hour": m["samples_per_hour"], "refinement_steps": 2,
+                      "chern_integers_identical_to_fp64": bool(np.array_equal(np.rint(cmx), np.rint(c64))),
+                      "max_chern_deviation_from_fp64": float(np.abs(cmx - c64).max()),
+                      "max_energy_rel_error_vs_fp64": float(np.abs(emx - e64).max() / np.abs(e64).max()),
+                      "kernel_ms_per_step": m["kernel_ms_per_step"]}}
+    ctx.close()
+    print(json.dumps(line), flush=True)
 
 
 def run_probe(args):
@@ -362,6 +461,10 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="hlm48x16", choices=["hlm48x16"] + sorted(RLM_WORKLOADS),
+                    help="hlm48x16 (default, the headline), or an rlm configuration (1 GPU, both precisions)")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision measurement on the same inputs")
     ap.add_argument("--probe", default=None, choices=["heevd"],
                     help="run one small eigensolver batch only (for profiler captures)")
     ap.add_argument("--n", type=int, default=256)
@@ -371,6 +474,8 @@ def main():
         run_probe(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.workload in RLM_WORKLOADS:
+        run_gpu_rlm(args)
     else:
         run_gpu(args)
 
