@@ -19,6 +19,7 @@
 // Every wait is a __syncthreads inside one CTA: no inter-CTA dependencies, no spins.
 #include "common.cuh"
 #include "small_eig.cuh"
+#include "zgemm.cuh"
 
 #include <cfloat>
 #include <cmath>
@@ -1016,133 +1017,139 @@ __global__ void k_z_to_x(const double* __restrict__ Z, C* __restrict__ X, int n,
     }
 }
 
-// W' = T (V^H X) for block j and 32 columns of X: grid (ceil(n/32), matrices).
-// Thread t owns W rows k0, k0+1 (k0 = 2*(t/8)) and columns c0..c0+3 (c0 = 4*(t%8)).
-template <class C>
-__global__ void __launch_bounds__(256)
-k_bt_w(const C* __restrict__ A, const C* __restrict__ Tw, const C* __restrict__ X,
-       C* __restrict__ Wp, int n, int j) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    typedef C VRow[BT_NB + 1];
-    typedef C CRow[33];
-    VRow* Vs = reinterpret_cast<VRow*>(smem_raw);          // [32][65]
-    CRow* Xs = reinterpret_cast<CRow*>(Vs + 32);           // [32][33]
-    CRow* Ws = Xs + 32;                                    // [64][33]
-    const int t = threadIdx.x;
-    const int k0 = 2 * (t / 8), c0 = 4 * (t % 8);
-    const size_t mat = blockIdx.y;
-    const int col0 = blockIdx.x * 32;
-    const C* a = A + mat * (size_t)n * n;
-    const C* x = X + mat * (size_t)n * n;
-    const int i0 = j * BT_NB, i1 = min(i0 + BT_NB - 1, n - 2);
-    C acc[2][4];
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = cz<C>();
-    for (int r0 = 0; r0 <= i1; r0 += 32) {
-        __syncthreads();
-        for (int idx = t; idx < 32 * BT_NB; idx += 256) {
-            const int rr = idx / BT_NB, k = idx % BT_NB;
-            Vs[rr][k] = r0 + rr <= i1 ? refl_entry(a, n, i0 + k, r0 + rr) : cz<C>();
-        }
-        for (int idx = t; idx < 32 * 32; idx += 256) {
-            const int cc = idx / 32, rr = idx % 32;   // coalesced along rows of column col0+cc
-            Xs[rr][cc] = (r0 + rr <= i1 && col0 + cc < n) ? x[(size_t)(col0 + cc) * n + r0 + rr] : cz<C>();
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int rr = 0; rr < 32; ++rr) {
-            const C va = Vs[rr][k0], vb = Vs[rr][k0 + 1];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const C xv = Xs[rr][c0 + v];
-                cfmac(acc[0][v], va, xv);
-                cfmac(acc[1][v], vb, xv);
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) Ws[k0 + u][c0 + v] = acc[u][v];
-    __syncthreads();
-    const int nblk = (n - 1 + BT_NB - 1) / BT_NB;
-    const C* T = Tw + (mat * nblk + j) * BT_NB * BT_NB;
-    C* wp = Wp + mat * (size_t)BT_NB * n;
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-        const int k = k0 + u;
-        C s[4] = {cz<C>(), cz<C>(), cz<C>(), cz<C>()};
-        for (int q = 0; q <= k; ++q) {
-            const C tq = T[k * BT_NB + q];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) cfma(s[v], tq, Ws[q][c0 + v]);
-        }
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
-            if (col0 + c0 + v < n) wp[(size_t)k * n + col0 + c0 + v] = s[v];
-    }
-}
+// ------------------------------------------------------------------ GEMM operands
+// Operand fills for k_zgemm (tiles [ZG_KC][BM + 1]); each writes every tile entry once,
+// in the order that is coalesced for the operand's memory layout.
 
-// X[0..i1][cols] -= V W' for block j: grid (row tiles of 64, column tiles of 32, matrices).
-// Thread t owns rows r0+2*(t/8)+{0,1} and columns c0..c0+3.
-template <class C>
-__global__ void __launch_bounds__(256)
-k_bt_upd(const C* __restrict__ A, const C* __restrict__ Wp, C* __restrict__ X, int n, int j) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    typedef C VRow[BT_NB + 1];
-    typedef C CRow[33];
-    VRow* Vs = reinterpret_cast<VRow*>(smem_raw);          // [64][65]
-    CRow* Ws = reinterpret_cast<CRow*>(Vs + 64);           // [64][33]
-    const int t = threadIdx.x;
-    const size_t mat = blockIdx.z;
-    const int row0 = blockIdx.x * 64, col0 = blockIdx.y * 32;
-    const int i0 = j * BT_NB, i1 = min(i0 + BT_NB - 1, n - 2);
-    if (row0 > i1) return;
-    const C* a = A + mat * (size_t)n * n;
-    const C* wp = Wp + mat * (size_t)BT_NB * n;
-    for (int idx = t; idx < 64 * BT_NB; idx += 256) {
-        const int rr = idx / BT_NB, k = idx % BT_NB;
-        Vs[rr][k] = row0 + rr <= i1 ? refl_entry(a, n, i0 + k, row0 + rr) : cz<C>();
-    }
-    for (int idx = t; idx < BT_NB * 32; idx += 256) {
-        const int k = idx / 32, cc = idx % 32;
-        Ws[k][cc] = col0 + cc < n ? wp[(size_t)k * n + col0 + cc] : cz<C>();
-    }
-    __syncthreads();
-    const int rl = 2 * (t / 8), c0 = 4 * (t % 8);
-    C s[2][4];
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) s[u][v] = cz<C>();
-#pragma unroll 4
-    for (int k = 0; k < BT_NB; ++k) {
-        const C va = Vs[rl][k], vb = Vs[rl + 1][k];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const C w = Ws[k][c0 + v];
-            cfma(s[0][v], va, w);
-            cfma(s[1][v], vb, w);
-        }
-    }
-    C* x = X + mat * (size_t)n * n;
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-        const int r = row0 + rl + u;
-        if (r > i1) continue;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int c = col0 + c0 + v;
-            if (c < n) {
-                C* p = &x[(size_t)c * n + r];
-                *p = csub(*p, s[u][v]);
+// A = H, Hermitian, from the upper triangle of column-major a ('U', imaginary diagonal
+// ignored): entries on and above the diagonal down their column, those below (disjoint)
+// along their row.
+struct OpHerm {
+    const cplx* a;
+    int n;
+    template <int BM>
+    __device__ __forceinline__ void fill(cplx (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
+        const cplx* am = a + mat * (size_t)n * n;
+        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
+            const int kk = idx / BM, rr = idx % BM, r = r0 + rr, k = k0 + kk;
+            if (r >= M || k >= K) {
+                s[kk][rr] = mk(0, 0);
+            } else if (r <= k) {
+                cplx h = am[(size_t)k * n + r];
+                if (r == k) h.y = 0.0;
+                s[kk][rr] = h;
             }
         }
+        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
+            const int rr = idx / ZG_KC, kk = idx % ZG_KC, r = r0 + rr, k = k0 + kk;
+            if (r < M && k < K && r > k) s[kk][rr] = cconj(am[(size_t)r * n + k]);
+        }
     }
-}
+};
+
+// A(r, k) = P(r, k) of a column-major P (entry at p[k*ld + r]): r fastest.
+template <class C, class PT>
+struct OpColA {
+    const PT* p;
+    int ld;
+    size_t stride;
+    template <int BM>
+    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
+        const PT* pm = p + mat * stride;
+        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
+            const int kk = idx / BM, rr = idx % BM, r = r0 + rr, k = k0 + kk;
+            s[kk][rr] = (r < M && k < K) ? from_c64<C>(to_c64(pm[(size_t)k * ld + r])) : cz<C>();
+        }
+    }
+};
+
+// A(r, k) = P(k, r) (conjugated if CONJ) of a column-major P (entry (k, r) at p[r*ld + k]):
+// the (conjugate) transpose, k fastest.
+template <class C, class PT, bool CONJ>
+struct OpRowA {
+    const PT* p;
+    int ld;
+    size_t stride;
+    template <int BM>
+    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
+        const PT* pm = p + mat * stride;
+        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
+            const int rr = idx / ZG_KC, kk = idx % ZG_KC, r = r0 + rr, k = k0 + kk;
+            C v = cz<C>();
+            if (r < M && k < K) {
+                v = from_c64<C>(to_c64(pm[(size_t)r * ld + k]));
+                if (CONJ) v.y = -v.y;
+            }
+            s[kk][rr] = v;
+        }
+    }
+};
+
+// B(k, c) = P(k, c) of a column-major P (entry at p[c*ld + k]): k fastest.
+template <class C, class PT>
+struct OpColB {
+    const PT* p;
+    int ld;
+    size_t stride;
+    __device__ __forceinline__ void fill(C (*s)[ZG_BN + 1], size_t mat, int k0, int c0, int K, int N) const {
+        const PT* pm = p + mat * stride;
+        for (int idx = threadIdx.x; idx < ZG_BN * ZG_KC; idx += 256) {
+            const int cc = idx / ZG_KC, kk = idx % ZG_KC, c = c0 + cc, k = k0 + kk;
+            s[kk][cc] = (c < N && k < K) ? from_c64<C>(to_c64(pm[(size_t)c * ld + k])) : cz<C>();
+        }
+    }
+};
+
+// Reflectors i0 + q of a reduced matrix as columns of V (V(r, q) = v_{i0+q}[r], with the
+// implicit 1 and the zeros): OpRefl gives A = V (r fastest), OpReflH gives A = V^H.
+template <class C>
+struct OpRefl {
+    const C* a;
+    int n, i0;
+    template <int BM>
+    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
+        const C* am = a + mat * (size_t)n * n;
+        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
+            const int kk = idx / BM, rr = idx % BM, r = r0 + rr, q = k0 + kk;
+            s[kk][rr] = (r < M && q < K) ? refl_entry(am, n, i0 + q, r) : cz<C>();
+        }
+    }
+};
+template <class C>
+struct OpReflH {
+    const C* a;
+    int n, i0;
+    template <int BM>
+    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
+        const C* am = a + mat * (size_t)n * n;
+        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
+            const int rr = idx / ZG_KC, kk = idx % ZG_KC, q = r0 + rr, r = k0 + kk;
+            C v = (q < M && r < K) ? refl_entry(am, n, i0 + q, r) : cz<C>();
+            v.y = -v.y;
+            s[kk][rr] = v;
+        }
+    }
+};
+
+// Epilogues
+template <class C>
+struct EpStore {   // P(r, c) = acc, column-major P with leading dimension ld
+    C* p;
+    int ld;
+    size_t stride;
+    __device__ __forceinline__ void store(size_t mat, int r, int c, C acc) const {
+        p[mat * stride + (size_t)c * ld + r] = acc;
+    }
+};
+template <class C>
+struct EpSub {     // X(r, c) -= acc
+    C* x;
+    int n;
+    __device__ __forceinline__ void store(size_t mat, int r, int c, C acc) const {
+        C* q = x + mat * (size_t)n * n + (size_t)c * n + r;
+        *q = csub(*q, acc);
+    }
+};
 
 // ------------------------------------------------- mixed mode: FP64 refinement kernels
 // The mixed mode reduces and back-transforms in single precision (k_hetrd<.., float>,
@@ -1159,107 +1166,90 @@ k_bt_upd(const C* __restrict__ A, const C* __restrict__ Wp, C* __restrict__ X, i
 // X F is a first-order correction of the size of the current error, so a single-precision
 // product carries it; R, E and the diagonal need double.  Each step roughly squares the
 // relative error of the vectors.
-// Eigenvalues closer than 2^-17 of the spectral radius are not separated by the single
-// precision start: chains of such gaps form clusters (k_ref_clusters).  Inside a cluster
-// of at most RF_KMAX members the vectors are re-resolved by a Rayleigh-Ritz step on the
-// cluster's subspace in double (k_ref_cluster_solve: S = X_C^H H X_C = E_CC + G_CC Lambda,
-// G_CC = X_C^H X_C, S y = mu G y; k_ref_cluster_apply: X_C <- X_C Y, lambda_C <- mu).
-// Larger clusters, and pairs whose gap is within 8 |E_ij| (first-order theory would not
-// hold), are orthogonalised only, F_ij = -(x_i^H x_j)/2, and keep Rayleigh quotients.
-static constexpr int RF_T = 64;    // output tile edge
-static constexpr int RF_K = 16;    // inner-dimension step
-static constexpr int RF_KMAX = 8;  // largest cluster resolved by Rayleigh-Ritz
-static constexpr double RF_CLUSTER = 0x1p-17;   // relative gap below which pairs cluster
+// Two neighbouring eigenpairs whose gap is within 8 x their residual norms ||r_j|| are not
+// separated by the current vectors (first-order theory needs |x_i^H r_j| << gap), and for
+// gaps below 2^-14 of the spectral radius the first-order correction cannot restore
+// orthogonality to double precision (its error is ~ u ||H|| / gap; LAPACK's inverse
+// iteration likewise re-orthogonalises eigenvalues closer than 1e-3 ||T||, dstein): chains
+// of such gaps form clusters (k_ref_clusters).  Inside a cluster of at most RF_KMAX members the vectors are re-resolved
+// by a Rayleigh-Ritz step on the cluster's subspace in double (k_ref_cluster_solve: S =
+// X_C^H H X_C = E_CC + G_CC Lambda, G_CC = X_C^H X_C, S y = mu G y; k_ref_cluster_apply:
+// X_C <- X_C Y, lambda_C <- mu).  Larger clusters, and any other pair whose gap is within
+// 8 |E_ij|, are orthogonalised only, F_ij = -(x_i^H x_j)/2, and keep Rayleigh quotients.
+static constexpr int RF_KMAX = 16;             // largest cluster resolved by Rayleigh-Ritz
+static constexpr double RF_RES = 8.0;          // gap / residual ratio below which pairs cluster
+static constexpr double RF_CLUSTER = 0x1p-14;  // relative gap below which pairs cluster
 
-// R = H X - X diag(lambda): grid (n/64 row tiles, n/64 column tiles, matrices).  Thread
-// t owns rows 4*(t/16)+{0..3} and columns (t%16) + 16*{0..3} of the tile.  H is read from
-// the upper triangle of A (column-major, 'U'), the diagonal's imaginary part ignored.
+// R = H X - X diag(lambda): epilogue of the GEMM H X (k_zgemm with OpHerm, OpColB).
 template <class XT>
-__global__ void __launch_bounds__(256)
-k_ref_resid(const cplx* __restrict__ A, const XT* __restrict__ X, const double* __restrict__ W,
-            cplx* __restrict__ Res, int n) {
-    __shared__ cplx Hs[RF_K][RF_T + 1];
-    __shared__ cplx Xs[RF_K][RF_T + 1];
-    const int t = threadIdx.x, tr = t / 16, tc = t % 16;
-    const size_t mat = blockIdx.z;
-    const int r0 = blockIdx.x * RF_T, c0 = blockIdx.y * RF_T;
-    const cplx* a = A + mat * (size_t)n * n;
-    const XT* x = X + mat * (size_t)n * n;
-    cplx acc[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = mk(0, 0);
-    for (int k0 = 0; k0 < n; k0 += RF_K) {
-        __syncthreads();
-        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
-            // on and above the diagonal: down the column (r fastest)
-            const int kk = idx / RF_T, rr = idx % RF_T;
-            const int r = r0 + rr, k = k0 + kk;
-            if (r >= n || k >= n) {
-                Hs[kk][rr] = mk(0, 0);
-            } else if (r <= k) {
-                cplx h = a[(size_t)k * n + r];
-                if (r == k) h.y = 0.0;
-                Hs[kk][rr] = h;
-            }
-        }
-        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
-            // below the diagonal (disjoint entries): along the row (k fastest)
-            const int rr = idx / RF_K, kk = idx % RF_K;
-            const int r = r0 + rr, k = k0 + kk;
-            if (r < n && k < n && r > k) Hs[kk][rr] = cconj(a[(size_t)r * n + k]);
-        }
-        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
-            const int cc = idx / RF_K, kk = idx % RF_K;
-            const int c = c0 + cc, k = k0 + kk;
-            Xs[kk][cc] = (c < n && k < n) ? to_c64(x[(size_t)c * n + k]) : mk(0, 0);
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < RF_K; ++kk) {
-            cplx hv[4], xv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) hv[u] = Hs[kk][4 * tr + u];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) xv[v] = Xs[kk][tc + 16 * v];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) cfma(acc[u][v], hv[u], xv[v]);
-        }
+struct EpResid {
+    const XT* x;
+    const double* w;
+    cplx* res;
+    int n;
+    __device__ __forceinline__ void store(size_t mat, int r, int c, cplx acc) const {
+        const size_t o = mat * (size_t)n * n + (size_t)c * n + r;
+        const cplx xr = to_c64(x[o]);
+        const double lam = w[mat * n + c];
+        res[o] = mk(acc.x - lam * xr.x, acc.y - lam * xr.y);
     }
-    cplx* res = Res + mat * (size_t)n * n;
-    const double* w = W + mat * n;
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        const int c = c0 + tc + 16 * v;
-        if (c >= n) continue;
-        const double lam = w[c];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int r = r0 + 4 * tr + u;
-            if (r >= n) continue;
-            const cplx xr = to_c64(x[(size_t)c * n + r]);
-            res[(size_t)c * n + r] = mk(acc[u][v].x - lam * xr.x, acc[u][v].y - lam * xr.y);
-        }
+};
+
+// Per eigenvector j (one warp each), in double: G_jj = x_j^H x_j, q_j = Re(x_j^H r_j) and
+// ||r_j||, stored as ST[3 (mat n + j) + {0, 1, 2}].
+template <class XT>
+__global__ void k_ref_colstats(const XT* __restrict__ X, const cplx* __restrict__ Res, double* __restrict__ ST,
+                               int n, int nmat) {
+    const int lane = threadIdx.x & 31;
+    const size_t gw = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (gw >= (size_t)nmat * n) return;
+    const size_t mat = gw / n;
+    const int j = (int)(gw % n);
+    const XT* x = X + mat * (size_t)n * n + (size_t)j * n;
+    const cplx* r = Res + mat * (size_t)n * n + (size_t)j * n;
+    double g = 0.0, q = 0.0, rr = 0.0;
+    for (int k = lane; k < n; k += 32) {
+        const cplx xv = to_c64(x[k]), rv = r[k];
+        g += xv.x * xv.x + xv.y * xv.y;
+        q += xv.x * rv.x + xv.y * rv.y;
+        rr += rv.x * rv.x + rv.y * rv.y;
+    }
+    g = warp_sum(g);
+    q = warp_sum(q);
+    rr = warp_sum(rr);
+    if (lane == 0) {
+        ST[3 * gw] = g;
+        ST[3 * gw + 1] = q;
+        ST[3 * gw + 2] = sqrt(rr);
     }
 }
 
 // Clusters of the ascending eigenvalues of each matrix (one thread per matrix): chains of
-// consecutive gaps <= RF_CLUSTER * spectral radius.  cl[j] = (first index, size).
-__global__ void k_ref_clusters(const double* __restrict__ W, int2* __restrict__ cl, int n, int nmat) {
+// consecutive pairs with gap <= RF_RES * max(||r||/||x||) or <= RF_CLUSTER * spectral radius.
+// cl[j] = (first index, size).
+__global__ void k_ref_clusters(const double* __restrict__ W, const double* __restrict__ ST, int2* __restrict__ cl,
+                               int n, int nmat) {
     const int mat = blockIdx.x * blockDim.x + threadIdx.x;
     if (mat >= nmat) return;
     const double* w = W + (size_t)mat * n;
+    const double* st = ST + (size_t)mat * n * 3;
     int2* c = cl + (size_t)mat * n;
-    const double tau = RF_CLUSTER * fmax(fabs(w[0]), fabs(w[n - 1]));
+    const double tie = RF_CLUSTER * fmax(fabs(w[0]), fabs(w[n - 1]));
     int a = 0;
+    double rho_prev = st[2] / sqrt(fmax(st[0], DBL_MIN));
     for (int j = 1; j <= n; ++j) {
-        if (j == n || w[j] - w[j - 1] > tau) {
+        bool split = true;
+        double rho = 0.0;
+        if (j < n) {
+            rho = st[3 * j + 2] / sqrt(fmax(st[3 * j], DBL_MIN));
+            const double gap = w[j] - w[j - 1];
+            split = gap > tie && gap > RF_RES * fmax(rho, rho_prev);
+        }
+        if (split) {
             for (int m = a; m < j; ++m) c[m] = make_int2(a, j - a);
             a = j;
         }
+        rho_prev = rho;
     }
 }
 
@@ -1273,78 +1263,38 @@ __device__ __forceinline__ cplx col_dot(const XT* __restrict__ xi, const XT* __r
 
 // F_ij = (X^H R)_ij / (lambda_j - lambda_i) for i != j; zero on the diagonal (set by
 // k_ref_diag) and inside Rayleigh-Ritz clusters; -(x_i^H x_j)/2 inside larger clusters and
-// for pairs too close for a first-order correction.  The products are taken in double:
-// F + F^H must cancel the orthogonality defect (E_ij - conj(E_ji) = (lambda_i - lambda_j)
-// x_i^H x_j).
+// for pairs too close for a first-order correction.  Epilogue of the GEMM X^H R taken in
+// double: F + F^H must cancel the orthogonality defect (E_ij - conj(E_ji) = (lambda_i -
+// lambda_j) x_i^H x_j).
 template <class XT>
-__global__ void __launch_bounds__(256)
-k_ref_coupling(const XT* __restrict__ X, const cplx* __restrict__ Res, const double* __restrict__ W,
-               const int2* __restrict__ CL, cplxf* __restrict__ F, int n) {
-    __shared__ cplx Xs[RF_K][RF_T + 1];
-    __shared__ cplx Rs[RF_K][RF_T + 1];
-    const int t = threadIdx.x, tr = t / 16, tc = t % 16;
-    const size_t mat = blockIdx.z;
-    const int i0 = blockIdx.x * RF_T, j0 = blockIdx.y * RF_T;
-    const XT* x = X + mat * (size_t)n * n;
-    const cplx* res = Res + mat * (size_t)n * n;
-    cplx acc[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = mk(0, 0);
-    for (int k0 = 0; k0 < n; k0 += RF_K) {
-        __syncthreads();
-        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
-            const int cc = idx / RF_K, kk = idx % RF_K;
-            const int k = k0 + kk;
-            Xs[kk][cc] = (i0 + cc < n && k < n) ? to_c64(x[(size_t)(i0 + cc) * n + k]) : mk(0, 0);
-            Rs[kk][cc] = (j0 + cc < n && k < n) ? res[(size_t)(j0 + cc) * n + k] : mk(0, 0);
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < RF_K; ++kk) {
-            cplx xv[4], rv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) xv[u] = Xs[kk][4 * tr + u];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) rv[v] = Rs[kk][tc + 16 * v];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) cfmac(acc[u][v], xv[u], rv[v]);
-        }
-    }
-    const double* w = W + mat * n;
-    const int2* cl = CL + mat * n;
-    cplxf* f = F + mat * (size_t)n * n;
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        const int j = j0 + tc + 16 * v;
-        if (j >= n) continue;
-        const double lj = w[j];
-        const int2 cj = cl[j];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int i = i0 + 4 * tr + u;
-            if (i >= n) continue;
-            cplxf val = make_float2(0.f, 0.f);
-            if (i != j) {
-                const double gap = lj - w[i];
-                const bool same = cl[i].x == cj.x;
-                if (same && cj.y <= RF_KMAX) {
-                    val = make_float2(0.f, 0.f);   // resolved by k_ref_cluster_solve
-                } else if (!same && fabs(gap) > 8.0 * sqrt(cabs2(acc[u][v]))) {
-                    const double ig = 1.0 / gap;
-                    val = make_float2((float)(acc[u][v].x * ig), (float)(acc[u][v].y * ig));
-                } else {
-                    const cplx g = col_dot(x + (size_t)i * n, x + (size_t)j * n, n);
-                    val = make_float2((float)(-0.5 * g.x), (float)(-0.5 * g.y));
-                }
+struct EpCoupling {
+    const XT* x;
+    const double* w;
+    const int2* cl;
+    cplxf* f;
+    int n;
+    __device__ __forceinline__ void store(size_t mat, int i, int j, cplx acc) const {
+        cplxf val = make_float2(0.f, 0.f);
+        if (i != j) {
+            const double* wm = w + mat * n;
+            const int2* cm_ = cl + mat * n;
+            const double gap = wm[j] - wm[i];
+            const int2 cj = cm_[j];
+            const bool same = cm_[i].x == cj.x;
+            if (same && cj.y <= RF_KMAX) {
+                val = make_float2(0.f, 0.f);   // resolved by k_ref_cluster_solve
+            } else if (!same && fabs(gap) > 8.0 * sqrt(cabs2(acc))) {
+                const double ig = 1.0 / gap;
+                val = make_float2((float)(acc.x * ig), (float)(acc.y * ig));
+            } else {
+                const XT* xm = x + mat * (size_t)n * n;
+                const cplx g = col_dot(xm + (size_t)i * n, xm + (size_t)j * n, n);
+                val = make_float2((float)(-0.5 * g.x), (float)(-0.5 * g.y));
             }
-            f[(size_t)j * n + i] = val;
         }
+        f[mat * (size_t)n * n + (size_t)j * n + i] = val;
     }
-}
+};
 
 // Rayleigh-Ritz on each cluster of 2..RF_KMAX members (one warp per cluster, found at its
 // first index): G = X_C^H X_C and E = X_C^H R_C by warp sums in double, S = E + G Lambda
@@ -1460,95 +1410,39 @@ __global__ void k_ref_cluster_solve(const XT* __restrict__ X, const cplx* __rest
     }
 }
 
-// Per eigenvector j (one warp each): G_jj = x_j^H x_j and Re(x_j^H r_j) in double;
-// lambda_j += Re(x_j^H r_j) / G_jj (Rayleigh quotient), F_jj = (1 - G_jj) / 2 -- except
-// for members of Rayleigh-Ritz clusters (F_jj = 0, lambda from k_ref_cluster_apply).
-template <class XT>
-__global__ void k_ref_diag(const XT* __restrict__ X, const cplx* __restrict__ Res, const int2* __restrict__ CL,
-                           double* __restrict__ W, cplxf* __restrict__ F, int n, int nmat) {
-    const int lane = threadIdx.x & 31;
-    const size_t gw = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    if (gw >= (size_t)nmat * n) return;
-    const size_t mat = gw / n;
-    const int j = (int)(gw % n);
-    const int2 c = CL[gw];
+// Per eigenvector j (one thread each): lambda_j += q_j / G_jj (Rayleigh quotient) and
+// F_jj = (1 - G_jj) / 2 from k_ref_colstats -- except for members of Rayleigh-Ritz clusters
+// (F_jj = 0, lambda from k_ref_cluster_apply).
+__global__ void k_ref_diag(const double* __restrict__ ST, const int2* __restrict__ CL, double* __restrict__ W,
+                           cplxf* __restrict__ F, int n, int nmat) {
+    const size_t gj = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gj >= (size_t)nmat * n) return;
+    const size_t mat = gj / n;
+    const int j = (int)(gj % n);
+    const int2 c = CL[gj];
     cplxf* fjj = F + mat * (size_t)n * n + (size_t)j * n + j;
     if (c.y >= 2 && c.y <= RF_KMAX) {
-        if (lane == 0) *fjj = make_float2(0.f, 0.f);
+        *fjj = make_float2(0.f, 0.f);
         return;
     }
-    const XT* x = X + mat * (size_t)n * n + (size_t)j * n;
-    const cplx* r = Res + mat * (size_t)n * n + (size_t)j * n;
-    double g = 0.0, q = 0.0;
-    for (int k = lane; k < n; k += 32) {
-        const cplx xv = to_c64(x[k]), rv = r[k];
-        g += xv.x * xv.x + xv.y * xv.y;
-        q += xv.x * rv.x + xv.y * rv.y;
-    }
-    g = warp_sum(g);
-    q = warp_sum(q);
-    if (lane == 0) {
-        W[mat * n + j] += q / g;
-        *fjj = make_float2((float)(0.5 * (1.0 - g)), 0.f);
-    }
+    const double g = ST[3 * gj], q = ST[3 * gj + 1];
+    W[gj] += q / g;
+    *fjj = make_float2((float)(0.5 * (1.0 - g)), 0.f);
 }
 
-// X_out = X + X F (single-precision product, double sum) into a separate buffer.
+// X_out = X + X F: epilogue of the single-precision GEMM X F, sum in double, into a
+// buffer other than X.
 template <class XT>
-__global__ void __launch_bounds__(256)
-k_ref_update(const XT* __restrict__ X, const cplxf* __restrict__ F, cplx* __restrict__ Out, int n) {
-    __shared__ cplxf Xs[RF_K][RF_T + 1];
-    __shared__ cplxf Fs[RF_K][RF_T + 1];
-    const int t = threadIdx.x, tr = t / 16, tc = t % 16;
-    const size_t mat = blockIdx.z;
-    const int r0 = blockIdx.x * RF_T, c0 = blockIdx.y * RF_T;
-    const XT* x = X + mat * (size_t)n * n;
-    const cplxf* f = F + mat * (size_t)n * n;
-    cplxf acc[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = make_float2(0.f, 0.f);
-    for (int k0 = 0; k0 < n; k0 += RF_K) {
-        __syncthreads();
-        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
-            const int kk = idx / RF_T, rr = idx % RF_T;    // X(r, k): r fastest
-            const int r = r0 + rr, k = k0 + kk;
-            Xs[kk][rr] = (r < n && k < n) ? from_c64<cplxf>(to_c64(x[(size_t)k * n + r])) : make_float2(0.f, 0.f);
-        }
-        for (int idx = t; idx < RF_K * RF_T; idx += 256) {
-            const int cc = idx / RF_K, kk = idx % RF_K;    // F(k, c): k fastest
-            const int c = c0 + cc, k = k0 + kk;
-            Fs[kk][cc] = (c < n && k < n) ? f[(size_t)c * n + k] : make_float2(0.f, 0.f);
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < RF_K; ++kk) {
-            cplxf xv[4], fv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) xv[u] = Xs[kk][4 * tr + u];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) fv[v] = Fs[kk][tc + 16 * v];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) cfma(acc[u][v], xv[u], fv[v]);
-        }
+struct EpUpdate {
+    const XT* x;
+    cplx* out;
+    int n;
+    __device__ __forceinline__ void store(size_t mat, int r, int c, cplxf acc) const {
+        const size_t o = mat * (size_t)n * n + (size_t)c * n + r;
+        const cplx xr = to_c64(x[o]);
+        out[o] = mk(xr.x + (double)acc.x, xr.y + (double)acc.y);
     }
-    cplx* out = Out + mat * (size_t)n * n;
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        const int c = c0 + tc + 16 * v;
-        if (c >= n) continue;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int r = r0 + 4 * tr + u;
-            if (r >= n) continue;
-            const cplx xr = to_c64(x[(size_t)c * n + r]);
-            out[(size_t)c * n + r] = mk(xr.x + (double)acc[u][v].x, xr.y + (double)acc[u][v].y);
-        }
-    }
-}
+};
 
 // X_C <- X_C Y and lambda_C <- mu for every Rayleigh-Ritz cluster (one warp per cluster,
 // rows dealt to lanes; every row is read before it is written, so in place).
@@ -1635,7 +1529,7 @@ struct HeevPlan {
     size_t smem_orm;
     int nblk16, nblk64;
     size_t off_d, off_e, off_tau, off_a, off_z, off_lu, off_x, off_t, off_w, off_res, off_x1, off_cl,
-        off_y, off_mu, per;
+        off_y, off_mu, off_st, per;
 };
 
 static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
@@ -1668,12 +1562,13 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     p.off_lu = off; off += r256(5 * (size_t)n * TRI_THREADS * sizeof(double));
     p.off_x = off; off += r256(nn * ce);
     p.off_t = off; off += r256((p.small_bt ? (size_t)p.nblk16 * ORM_NB * ORM_NB : (size_t)p.nblk64 * BT_NB * BT_NB) * ce);
-    p.off_w = off; off += p.small_bt ? 0 : r256((size_t)BT_NB * n * ce);
+    p.off_w = off; off += p.small_bt ? 0 : r256(2 * (size_t)BT_NB * n * ce);   // G and W' of a block
     p.off_res = off; off += mixed ? r256(nn * sizeof(cplx)) : 0;
     p.off_x1 = off; off += p.refine_steps >= 2 ? r256(nn * sizeof(cplx)) : 0;   // step-1 vectors
     p.off_cl = off; off += mixed ? r256(n * sizeof(int2)) : 0;
     p.off_y = off; off += mixed ? r256((size_t)n * RF_KMAX * sizeof(cplx)) : 0;
     p.off_mu = off; off += mixed ? r256(n * sizeof(double)) : 0;
+    p.off_st = off; off += mixed ? r256(3 * (size_t)n * sizeof(double)) : 0;
     p.per = off;
     return p;
 }
@@ -1722,11 +1617,7 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         return RLMB_OK;
     }
     const size_t smem_t = 2 * BT_NB * BT_NB * sizeof(C);
-    const size_t smem_w = (32 * (BT_NB + 1) + 32 * 33 + BT_NB * 33) * sizeof(C);
-    const size_t smem_u = (64 * (BT_NB + 1) + BT_NB * 33) * sizeof(C);
-    if (cudaFuncSetAttribute(k_larft64<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess ||
-        cudaFuncSetAttribute(k_bt_w<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w) != cudaSuccess ||
-        cudaFuncSetAttribute(k_bt_upd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_u) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_larft64<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_PROF("k_larft");
     k_larft64<R><<<dim3(p.nblk64, nb), 256, smem_t, st>>>(Aw, TAUw, Tw, n);
@@ -1734,13 +1625,29 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
     RLMB_CHUNK_PROF("k_ormtr");
     k_z_to_x<C><<<2048, 256, 0, st>>>(Zw, Xw, n, (size_t)nb * nn);
     RLMB_CHUNK_LAUNCHED();
+    // per block j of 64 reflectors (zlarfb): G = V^H X, W' = T G, X -= V W'; G and W' are
+    // [n][64] per matrix (column c of G at c*64)
+    C* G = Wp;
+    C* W2 = Wp + (size_t)nb * BT_NB * n;
+    const size_t gs = (size_t)BT_NB * n;
     for (int j = 0; j < p.nblk64; ++j) {
-        const int i1 = std::min(j * BT_NB + BT_NB - 1, n - 2);
+        const int i0 = j * BT_NB;
+        const int rows = std::min(i0 + BT_NB - 1, n - 2) + 1;   // rows 0..i1 carry the block
         RLMB_CHUNK_PROF("k_ormtr");
-        k_bt_w<C><<<dim3((n + 31) / 32, nb), 256, smem_w, st>>>(Aw, Tw, Xw, Wp, n, j);
+        if (launch_zgemm<C, 64>(st, OpReflH<C>{Aw, n, i0}, OpColB<C, C>{Xw, n, nn}, EpStore<C>{G, BT_NB, gs},
+                                BT_NB, n, rows, nb) != cudaSuccess)
+            return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
         RLMB_CHUNK_PROF("k_ormtr");
-        k_bt_upd<C><<<dim3(i1 / 64 + 1, (n + 31) / 32, nb), 256, smem_u, st>>>(Aw, Wp, Xw, n, j);
+        if (launch_zgemm<C, 64>(st, OpRowA<C, C, false>{Tw + (size_t)j * BT_NB * BT_NB, BT_NB,
+                                                        (size_t)p.nblk64 * BT_NB * BT_NB},
+                                OpColB<C, C>{G, BT_NB, gs}, EpStore<C>{W2, BT_NB, gs}, BT_NB, n, BT_NB, nb) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        RLMB_CHUNK_LAUNCHED();
+        RLMB_CHUNK_PROF("k_ormtr");
+        if (launch_zgemm<C, 128>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs}, EpSub<C>{Xw, n},
+                                 rows, n, BT_NB, nb) != cudaSuccess)
+            return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
     }
     return RLMB_OK;
@@ -1749,27 +1656,36 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
 // One refinement step from the vectors X (single or double) to Out (double, not X).
 template <class XT>
 static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const cplx* A, const XT* X,
-                       double* W, cplx* Res, cplxf* F, int2* CL, cplx* YB, double* MU, cplx* Out,
-                       long long* launches) {
-    const dim3 g((n + RF_T - 1) / RF_T, (n + RF_T - 1) / RF_T, nb);
+                       double* W, cplx* Res, cplxf* F, int2* CL, cplx* YB, double* MU, double* ST,
+                       cplx* Out, long long* launches) {
+    const size_t nn = (size_t)n * n;
     const unsigned gw = (unsigned)(((size_t)nb * n + 7) / 8);   // one warp per column
     RLMB_CHUNK_PROF("k_ref_resid");
-    k_ref_resid<XT><<<g, 256, 0, st>>>(A, X, W, Res, n);
+    if (launch_zgemm<cplx, 64>(st, OpHerm{A, n}, OpColB<cplx, XT>{X, n, nn}, EpResid<XT>{X, W, Res, n},
+                                n, n, n, nb) != cudaSuccess)
+        return RLMB_ERR_CUDA;
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_colstats");
+    k_ref_colstats<XT><<<gw, 256, 0, st>>>(X, Res, ST, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_clusters");
-    k_ref_clusters<<<(nb + 127) / 128, 128, 0, st>>>(W, CL, n, nb);
+    k_ref_clusters<<<(nb + 127) / 128, 128, 0, st>>>(W, ST, CL, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_coupling");
-    k_ref_coupling<XT><<<g, 256, 0, st>>>(X, Res, W, CL, F, n);
+    if (launch_zgemm<cplx, 64>(st, OpRowA<cplx, XT, true>{X, n, nn}, OpColB<cplx, cplx>{Res, n, nn},
+                                EpCoupling<XT>{X, W, CL, F, n}, n, n, n, nb) != cudaSuccess)
+        return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_cluster");
     k_ref_cluster_solve<XT><<<gw, 256, 0, st>>>(X, Res, W, CL, YB, MU, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_diag");
-    k_ref_diag<XT><<<gw, 256, 0, st>>>(X, Res, CL, W, F, n, nb);
+    k_ref_diag<<<(unsigned)(((size_t)nb * n + 255) / 256), 256, 0, st>>>(ST, CL, W, F, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_update");
-    k_ref_update<XT><<<g, 256, 0, st>>>(X, F, Out, n);
+    if (launch_zgemm<cplxf, 128>(st, OpColA<cplxf, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
+                                 EpUpdate<XT>{X, Out, n}, n, n, n, nb) != cudaSuccess)
+        return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_cluster");
     k_ref_cluster_apply<<<gw, 256, 0, st>>>(Out, CL, YB, MU, W, n, nb);
@@ -1824,6 +1740,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     int2* CL = reinterpret_cast<int2*>(base + p.off_cl * B);
     cplx* YB = reinterpret_cast<cplx*>(base + p.off_y * B);
     double* MU = reinterpret_cast<double*>(base + p.off_mu * B);
+    double* ST = reinterpret_cast<double*>(base + p.off_st * B);
     RLMB_CHUNK_PROF("k_to_single");
     k_to_single<<<2048, 256, 0, st>>>(A, As, B * nn);
     RLMB_CHUNK_LAUNCHED();
@@ -1840,11 +1757,11 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     // refinement: the single-precision copy of H is free now and holds F.  Step 1 starts
     // from the single-precision vectors, step 2 from step 1's double vectors (X1); the
     // last step writes the caller's buffer (every step's residual reads H first).
-    if (int rc = refine_step<cplxf>(ctx, st, n, nb, A, Xw, W, Res, As, CL, YB, MU,
+    if (int rc = refine_step<cplxf>(ctx, st, n, nb, A, Xw, W, Res, As, CL, YB, MU, ST,
                                     p.refine_steps >= 2 ? X1 : A, launches))
         return rc;
     if (p.refine_steps >= 2)
-        if (int rc = refine_step<cplx>(ctx, st, n, nb, A, X1, W, Res, As, CL, YB, MU, A, launches)) return rc;
+        if (int rc = refine_step<cplx>(ctx, st, n, nb, A, X1, W, Res, As, CL, YB, MU, ST, A, launches)) return rc;
     return RLMB_OK;
 }
 #undef RLMB_CHUNK_LAUNCHED

@@ -1,0 +1,96 @@
+// Batched complex GEMM tile engine (sm_100a, SIMT FP64 or FP32 FMA pipes).
+//
+// C = A B for every matrix of a batch (blockIdx.z), output tiles of BM x 64 per CTA of
+// 256 threads; thread t = 16 tr + tc owns rows RM*tr .. RM*tr+RM-1 (RM = BM/16) and
+// columns tc + 16 v (v < 4) of the tile: RM x 4 complex accumulators in registers, so that
+// every complex operand read from shared memory feeds 4 (A) or RM (B) multiply-adds.
+// The inner dimension advances KC at a time through two shared-memory stages: the next
+// stage is filled (global loads by all threads) while the current one is consumed.
+//
+// Operands are functors that fill shared-memory tiles in whatever order is coalesced for
+// their memory layout, writing every entry of the tile (zero outside the matrix):
+//   la.fill<BM>(As, mat, r0, k0, M, K):  As[kk][rr] = A(r0 + rr, k0 + kk), kk < KC, rr < BM
+//   lb.fill(Bs, mat, k0, c0, K, N):  Bs[kk][cc] = B(k0 + kk, c0 + cc), kk < KC, cc < 64
+// and the epilogue ep.store(mat, r, c, acc) is called once per output entry r < M, c < N.
+#pragma once
+#include "common.cuh"
+
+namespace rlmb {
+
+static constexpr int ZG_BN = 64;
+static constexpr int ZG_KC = 8;
+
+template <class C, int BM>
+struct ZgTiles {
+    C a[2][ZG_KC][BM + 1];
+    C b[2][ZG_KC][ZG_BN + 1];
+};
+
+template <class C, int BM, class LA, class LB, class EP>
+__global__ void __launch_bounds__(256, BM == 64 ? 2 : 1)
+k_zgemm(LA la, LB lb, EP ep, int M, int N, int K) {
+    constexpr int RM = BM / 16;
+    extern __shared__ __align__(16) unsigned char zg_smem[];
+    ZgTiles<C, BM>& s = *reinterpret_cast<ZgTiles<C, BM>*>(zg_smem);
+    const int t = threadIdx.x, tr = t / 16, tc = t % 16;
+    const size_t mat = blockIdx.z;
+    const int r0 = blockIdx.x * BM, c0 = blockIdx.y * ZG_BN;
+    C acc[RM][4];
+#pragma unroll
+    for (int u = 0; u < RM; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = cz<C>();
+    const int nk = (K + ZG_KC - 1) / ZG_KC;
+    if (nk > 0) {
+        la.template fill<BM>(s.a[0], mat, r0, 0, M, K);
+        lb.fill(s.b[0], mat, 0, c0, K, N);
+    }
+    __syncthreads();
+    for (int kt = 0; kt < nk; ++kt) {
+        const int cur = kt & 1;
+        if (kt + 1 < nk) {
+            la.template fill<BM>(s.a[cur ^ 1], mat, r0, (kt + 1) * ZG_KC, M, K);
+            lb.fill(s.b[cur ^ 1], mat, (kt + 1) * ZG_KC, c0, K, N);
+        }
+#pragma unroll
+        for (int kk = 0; kk < ZG_KC; ++kk) {
+            C av[RM], bv[4];
+#pragma unroll
+            for (int u = 0; u < RM; ++u) av[u] = s.a[cur][kk][RM * tr + u];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) bv[v] = s.b[cur][kk][tc + 16 * v];
+#pragma unroll
+            for (int u = 0; u < RM; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) cfma(acc[u][v], av[u], bv[v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int c = c0 + tc + 16 * v;
+        if (c >= N) continue;
+#pragma unroll
+        for (int u = 0; u < RM; ++u) {
+            const int r = r0 + RM * tr + u;
+            if (r < M) ep.store(mat, r, c, acc[u][v]);
+        }
+    }
+}
+
+template <class C, int BM>
+constexpr size_t zgemm_smem() { return sizeof(ZgTiles<C, BM>); }
+
+// Launch on a batch of nb matrices; returns the launch error.
+template <class C, int BM, class LA, class LB, class EP>
+cudaError_t launch_zgemm(cudaStream_t st, const LA& la, const LB& lb, const EP& ep, int M, int N, int K, int nb) {
+    auto kern = k_zgemm<C, BM, LA, LB, EP>;
+    const size_t smem = zgemm_smem<C, BM>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((M + BM - 1) / BM, (N + ZG_BN - 1) / ZG_BN, nb);
+    kern<<<grid, 256, smem, st>>>(la, lb, ep, M, N, K);
+    return cudaGetLastError();
+}
+
+}  // namespace rlmb
