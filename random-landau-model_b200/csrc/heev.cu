@@ -1018,118 +1018,95 @@ __global__ void k_z_to_x(const double* __restrict__ Z, C* __restrict__ X, int n,
 }
 
 // ------------------------------------------------------------------ GEMM operands
-// Operand fills for k_zgemm (tiles [ZG_KC][BM + 1]); each writes every tile entry once,
-// in the order that is coalesced for the operand's memory layout.
+// Element accessors for k_zgemm (A: elem(mat, r, k), B: elem(mat, k, c)).
 
-// A = H, Hermitian, from the upper triangle of column-major a ('U', imaginary diagonal
-// ignored): entries on and above the diagonal down their column, those below (disjoint)
-// along their row.
-struct OpHerm {
-    const cplx* a;
-    int n;
-    template <int BM>
-    __device__ __forceinline__ void fill(cplx (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
-        const cplx* am = a + mat * (size_t)n * n;
-        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
-            const int kk = idx / BM, rr = idx % BM, r = r0 + rr, k = k0 + kk;
-            if (r >= M || k >= K) {
-                s[kk][rr] = mk(0, 0);
-            } else if (r <= k) {
-                cplx h = am[(size_t)k * n + r];
-                if (r == k) h.y = 0.0;
-                s[kk][rr] = h;
-            }
-        }
-        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
-            const int rr = idx / ZG_KC, kk = idx % ZG_KC, r = r0 + rr, k = k0 + kk;
-            if (r < M && k < K && r > k) s[kk][rr] = cconj(am[(size_t)r * n + k]);
-        }
-    }
-};
-
-// A(r, k) = P(r, k) of a column-major P (entry at p[k*ld + r]): r fastest.
+// A(r, k) = P(r, k) of a column-major P (entry at p[k*ld + r]): r contiguous.
 template <class C, class PT>
 struct OpColA {
+    static constexpr bool RFAST = true;
     const PT* p;
     int ld;
     size_t stride;
-    template <int BM>
-    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
-        const PT* pm = p + mat * stride;
-        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
-            const int kk = idx / BM, rr = idx % BM, r = r0 + rr, k = k0 + kk;
-            s[kk][rr] = (r < M && k < K) ? from_c64<C>(to_c64(pm[(size_t)k * ld + r])) : cz<C>();
-        }
+    __device__ __forceinline__ C elem(size_t mat, int r, int k) const {
+        return from_c64<C>(to_c64(p[mat * stride + (size_t)k * ld + r]));
     }
 };
 
-// A(r, k) = P(k, r) (conjugated if CONJ) of a column-major P (entry (k, r) at p[r*ld + k]):
-// the (conjugate) transpose, k fastest.
+// A(r, k) = P(k, r), conjugated if CONJ, of a column-major P (entry (k, r) at p[r*ld + k]):
+// the (conjugate) transpose, k contiguous.
 template <class C, class PT, bool CONJ>
 struct OpRowA {
+    static constexpr bool RFAST = false;
     const PT* p;
     int ld;
     size_t stride;
-    template <int BM>
-    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
-        const PT* pm = p + mat * stride;
-        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
-            const int rr = idx / ZG_KC, kk = idx % ZG_KC, r = r0 + rr, k = k0 + kk;
-            C v = cz<C>();
-            if (r < M && k < K) {
-                v = from_c64<C>(to_c64(pm[(size_t)r * ld + k]));
-                if (CONJ) v.y = -v.y;
-            }
-            s[kk][rr] = v;
-        }
+    __device__ __forceinline__ C elem(size_t mat, int r, int k) const {
+        C v = from_c64<C>(to_c64(p[mat * stride + (size_t)r * ld + k]));
+        if (CONJ) v.y = -v.y;
+        return v;
     }
 };
 
-// B(k, c) = P(k, c) of a column-major P (entry at p[c*ld + k]): k fastest.
+// B(k, c) = P(k, c) of a column-major P (entry at p[c*ld + k]): k contiguous.
 template <class C, class PT>
 struct OpColB {
+    static constexpr bool KFAST = true;
     const PT* p;
     int ld;
     size_t stride;
-    __device__ __forceinline__ void fill(C (*s)[ZG_BN + 1], size_t mat, int k0, int c0, int K, int N) const {
-        const PT* pm = p + mat * stride;
-        for (int idx = threadIdx.x; idx < ZG_BN * ZG_KC; idx += 256) {
-            const int cc = idx / ZG_KC, kk = idx % ZG_KC, c = c0 + cc, k = k0 + kk;
-            s[kk][cc] = (c < N && k < K) ? from_c64<C>(to_c64(pm[(size_t)c * ld + k])) : cz<C>();
-        }
+    __device__ __forceinline__ C elem(size_t mat, int k, int c) const {
+        return from_c64<C>(to_c64(p[mat * stride + (size_t)c * ld + k]));
     }
 };
 
 // Reflectors i0 + q of a reduced matrix as columns of V (V(r, q) = v_{i0+q}[r], with the
-// implicit 1 and the zeros): OpRefl gives A = V (r fastest), OpReflH gives A = V^H.
+// implicit 1 and the zeros): OpRefl gives A = V (r contiguous), OpReflH A = V^H.
 template <class C>
 struct OpRefl {
+    static constexpr bool RFAST = true;
     const C* a;
     int n, i0;
-    template <int BM>
-    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
-        const C* am = a + mat * (size_t)n * n;
-        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
-            const int kk = idx / BM, rr = idx % BM, r = r0 + rr, q = k0 + kk;
-            s[kk][rr] = (r < M && q < K) ? refl_entry(am, n, i0 + q, r) : cz<C>();
-        }
+    __device__ __forceinline__ C elem(size_t mat, int r, int q) const {
+        return refl_entry(a + mat * (size_t)n * n, n, i0 + q, r);
     }
 };
 template <class C>
 struct OpReflH {
+    static constexpr bool RFAST = false;
     const C* a;
     int n, i0;
-    template <int BM>
-    __device__ __forceinline__ void fill(C (*s)[BM + 1], size_t mat, int r0, int k0, int M, int K) const {
-        const C* am = a + mat * (size_t)n * n;
-        for (int idx = threadIdx.x; idx < BM * ZG_KC; idx += 256) {
-            const int rr = idx / ZG_KC, kk = idx % ZG_KC, q = r0 + rr, r = k0 + kk;
-            C v = (q < M && r < K) ? refl_entry(am, n, i0 + q, r) : cz<C>();
-            v.y = -v.y;
-            s[kk][rr] = v;
-        }
+    __device__ __forceinline__ C elem(size_t mat, int q, int r) const {
+        C v = refl_entry(a + mat * (size_t)n * n, n, i0 + q, r);
+        v.y = -v.y;
+        return v;
     }
 };
+
+// Complete a Hermitian matrix stored in the upper triangle (column-major, 'U') in place:
+// lower triangle = conjugate of the upper, imaginary part of the diagonal zeroed.  Tiles of
+// 32 x 32 through shared memory, both sides coalesced; grid (n/32, n/32, matrices), only
+// tiles on or below the diagonal work.  Reads (strict upper) and writes (strict lower and
+// diagonal) never overlap.
+__global__ void k_herm_fill(cplx* __restrict__ A, int n) {
+    __shared__ cplx tile[32][33];
+    const int cb = blockIdx.x, rb = blockIdx.y;   // output tile: rows rb, columns cb
+    if (rb < cb) return;
+    cplx* a = A + (size_t)blockIdx.z * n * n;
+    const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8
+    // input: upper entries (c, r) at a[r*n + c] for r in block rb, c in block cb
+    for (int j = ty; j < 32; j += 8) {
+        const int r = rb * 32 + j, c = cb * 32 + tx;
+        if (r < n && c < n && c < r) tile[j][tx] = a[(size_t)r * n + c];
+    }
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+        const int c = cb * 32 + j, r = rb * 32 + tx;
+        if (r < n && c < n) {
+            if (r > c) a[(size_t)c * n + r] = cconj(tile[tx][j]);
+            else if (r == c) a[(size_t)c * n + r].y = 0.0;
+        }
+    }
+}
 
 // Epilogues
 template <class C>
@@ -1180,7 +1157,7 @@ static constexpr int RF_KMAX = 16;             // largest cluster resolved by Ra
 static constexpr double RF_RES = 8.0;          // gap / residual ratio below which pairs cluster
 static constexpr double RF_CLUSTER = 0x1p-14;  // relative gap below which pairs cluster
 
-// R = H X - X diag(lambda): epilogue of the GEMM H X (k_zgemm with OpHerm, OpColB).
+// R = H X - X diag(lambda): epilogue of the GEMM H X (H completed by k_herm_fill).
 template <class XT>
 struct EpResid {
     const XT* x;
@@ -1661,7 +1638,7 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const 
     const size_t nn = (size_t)n * n;
     const unsigned gw = (unsigned)(((size_t)nb * n + 7) / 8);   // one warp per column
     RLMB_CHUNK_PROF("k_ref_resid");
-    if (launch_zgemm<cplx, 64>(st, OpHerm{A, n}, OpColB<cplx, XT>{X, n, nn}, EpResid<XT>{X, W, Res, n},
+    if (launch_zgemm<cplx, 64>(st, OpColA<cplx, cplx>{A, n, nn}, OpColB<cplx, XT>{X, n, nn}, EpResid<XT>{X, W, Res, n},
                                 n, n, n, nb) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
@@ -1683,7 +1660,7 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const 
     k_ref_diag<<<(unsigned)(((size_t)nb * n + 255) / 256), 256, 0, st>>>(ST, CL, W, F, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_update");
-    if (launch_zgemm<cplxf, 128>(st, OpColA<cplxf, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
+    if (launch_zgemm<cplxf, 64>(st, OpColA<cplxf, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
                                  EpUpdate<XT>{X, Out, n}, n, n, n, nb) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
@@ -1741,6 +1718,9 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     cplx* YB = reinterpret_cast<cplx*>(base + p.off_y * B);
     double* MU = reinterpret_cast<double*>(base + p.off_mu * B);
     double* ST = reinterpret_cast<double*>(base + p.off_st * B);
+    RLMB_CHUNK_PROF("k_herm_fill");
+    k_herm_fill<<<dim3((n + 31) / 32, (n + 31) / 32, nb), dim3(32, 8), 0, st>>>(A, n);
+    RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_to_single");
     k_to_single<<<2048, 256, 0, st>>>(A, As, B * nn);
     RLMB_CHUNK_LAUNCHED();
