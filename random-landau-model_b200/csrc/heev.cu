@@ -194,7 +194,9 @@ __device__ __forceinline__ void reflector(const C alpha, R xnorm2, R& beta, C& t
 
 // Unblocked reduction A = Q T Q^H (zhetd2, uplo='U') with look-ahead: step i's rank-2
 // update and step i-1's matrix-vector product share one pass over the leading block.
-// a: n*n col-major (upper triangle), real type R (double, or float in the mixed mode).
+// a: n*n col-major (upper triangle), real type R (double, or float in the mixed mode); the
+// leading m x m block is reduced (m < n after the blocked panels of k_hetrd_panel, which
+// own E and TAU from index m - 1 on).
 // On exit column c (c >= 1) rows 0..c-2 hold the reflector of step c-1 (its entry c-1 is
 // 1 and not stored), D/E the tridiagonal (double) and TAU the reflector scalars.  The
 // leading block moves into shared memory once its packed upper triangle fits in
@@ -202,14 +204,14 @@ __device__ __forceinline__ void reflector(const C alpha, R xnorm2, R& beta, C& t
 template <int NT, class R>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 4)
 k_hetrd(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
-        typename Cx<R>::T* __restrict__ TAU, int n, int tri_cap) {
+        typename Cx<R>::T* __restrict__ TAU, int n, int m, int tri_cap) {
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* v = reinterpret_cast<C*>(smem_raw);   // [n] current reflector
-    C* w = v + n;                             // [n] its w vector
-    C* vn = w + n;                            // [n] next reflector / column buffer
-    C* pn = vn + n;                           // [n] A' vn accumulator
-    R* red = reinterpret_cast<R*>(pn + n);    // [2*warps]
+    C* v = reinterpret_cast<C*>(smem_raw);   // [m] current reflector
+    C* w = v + m;                             // [m] its w vector
+    C* vn = w + m;                            // [m] next reflector / column buffer
+    C* pn = vn + m;                           // [m] A' vn accumulator
+    R* red = reinterpret_cast<R*>(pn + m);    // [2*warps]
     C* tri = reinterpret_cast<C*>(red + 2 * (NT / 32));   // packed triangle
     const int tid = threadIdx.x;
     const size_t mat = blockIdx.x;
@@ -218,18 +220,20 @@ k_hetrd(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __res
     double* dd = D + mat * n;
     double* ee = E + mat * n;
     C* tt = TAU + mat * n;
-    if (n == 1) {
+    if (m == 1) {
         if (tid == 0) {
             dd[0] = gs.at(0, 0)->x;
-            ee[0] = 0.0;
-            tt[0] = cz<C>();
+            if (m == n) {
+                ee[0] = 0.0;
+                tt[0] = cz<C>();
+            }
         }
         return;
     }
     bool resident = false;
-    // -- prologue: reflector of step n-2 from column n-1, then p = A v over [0..n-2]^2
+    // -- prologue: reflector of step m-2 from column m-1, then p = A v over [0..m-2]^2
     {
-        const int i = n - 2;
+        const int i = m - 2;
         R part = 0;
         for (int r = tid; r <= i + 1; r += NT) {
             const C x = *gs.at(r, i + 1);
@@ -247,13 +251,13 @@ k_hetrd(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __res
             v[r] = x;
             *gs.at(r, i + 1) = x;
         }
-        for (int r = tid; r < n; r += NT) {
+        for (int r = tid; r < m; r += NT) {
             w[r] = cz<C>();
             pn[r] = cz<C>();
         }
         if (tid == 0) {
             v[i] = cm<C>(1, 0);
-            dd[n - 1] = vn[n - 1].x;
+            dd[m - 1] = vn[m - 1].x;
             *gs.at(i, i + 1) = cm<C>(beta, 0);
             ee[i] = beta;
             tt[i] = tau;
@@ -274,7 +278,7 @@ k_hetrd(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __res
     }
     // -- main loop: v, w belong to step i (column i+1 done); finish column i, build the
     //    reflector of step i-1 from it, then one fused pass over [0..i-1]^2
-    for (int i = n - 2; i >= 1; --i) {
+    for (int i = m - 2; i >= 1; --i) {
         if (!resident && (i + 1) * (i + 2) / 2 <= tri_cap) {
             // move the leading (i+1)x(i+1) upper triangle into shared memory
             for (int c = 0; c <= i; ++c)
@@ -339,8 +343,10 @@ k_hetrd(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __res
         C u = cmul(v[0], cconj(w[0]));
         cfma(u, w[0], cconj(v[0]));
         dd[0] = x.x - u.x;
-        ee[n - 1] = 0.0;
-        tt[n - 1] = cz<C>();
+        if (m == n) {
+            ee[n - 1] = 0.0;
+            tt[n - 1] = cz<C>();
+        }
     }
 }
 
@@ -1114,6 +1120,7 @@ struct EpStore {   // P(r, c) = acc, column-major P with leading dimension ld
     C* p;
     int ld;
     size_t stride;
+    __device__ __forceinline__ bool skip(int, int, int) const { return false; }
     __device__ __forceinline__ void store(size_t mat, int r, int c, C acc) const {
         p[mat * stride + (size_t)c * ld + r] = acc;
     }
@@ -1122,9 +1129,161 @@ template <class C>
 struct EpSub {     // X(r, c) -= acc
     C* x;
     int n;
+    __device__ __forceinline__ bool skip(int, int, int) const { return false; }
     __device__ __forceinline__ void store(size_t mat, int r, int c, C acc) const {
         C* q = x + mat * (size_t)n * n + (size_t)c * n + r;
         *q = csub(*q, acc);
+    }
+};
+
+// ------------------------------------------------------------- blocked k_hetrd (large n)
+// For large orders the reduction runs in panels of HP_W columns (LAPACK zlatrd + zher2k,
+// uplo='U', restated): k_hetrd_panel reduces columns m-1 .. m-HP_W of the leading m x m
+// block one CTA per matrix, keeping each column's reflector v and its w = tau A' v - ...
+// in the panel buffers V, W instead of updating the leading block: column c is first
+// brought up to date with the panel's earlier pairs, its matrix-vector product reads the
+// leading c x c block as stored (read only) and is corrected by the same pairs.  The
+// rank-2*HP_W update A -= V W^H + W V^H of the remaining leading block then runs as a GEMM
+// over all SMs (k_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
+// k_hetrd.  D, E, TAU and the reflector storage are those of the unblocked reduction.
+static constexpr int HP_W = 32;      // panel width
+static constexpr int HT_TAIL = 256;  // order below which the unblocked kernel finishes
+static constexpr int HT_BLOCKED_MIN = 640;   // orders from which the blocked reduction runs
+
+template <int NT, class R>
+__global__ void __launch_bounds__(NT, 1)
+k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
+              typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ PV,
+              typename Cx<R>::T* __restrict__ PW, int n, int m) {
+    typedef typename Cx<R>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* vn = reinterpret_cast<C*>(smem_raw);   // [m] column / reflector
+    C* pn = vn + m;                            // [m] A' v accumulator
+    C* coef = pn + m;                          // [2*HP_W] w_q^H v, v_q^H v
+    R* red = reinterpret_cast<R*>(coef + 2 * HP_W);   // [2*warps]
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const size_t mat = blockIdx.x;
+    GlobalStore<C> gs{A + mat * (size_t)n * n, n};
+    double* dd = D + mat * n;
+    double* ee = E + mat * n;
+    C* tt = TAU + mat * n;
+    C* V = PV + mat * (size_t)HP_W * n;   // pair q at V + q*n, W + q*n
+    C* W = PW + mat * (size_t)HP_W * n;
+    if (m == n && tid == 0) {
+        ee[n - 1] = 0.0;
+        tt[n - 1] = cz<C>();
+    }
+    for (int j = 0; j < HP_W; ++j) {
+        const int c = m - 1 - j;
+        // (1) column c brought up to date with the panel's pairs q < j
+        R part = 0;
+        for (int r = tid; r <= c; r += NT) {
+            C x = *gs.at(r, c);
+            for (int q = 0; q < j; ++q) {
+                const C* vq = V + (size_t)q * n;
+                const C* wq = W + (size_t)q * n;
+                C u = cmul(vq[r], cconj(wq[c]));
+                cfma(u, wq[r], cconj(vq[c]));
+                x = csub(x, u);
+            }
+            if (r == c) x.y = 0;
+            vn[r] = x;
+            if (r < c - 1) part += cabs2(x);
+            if (r < c) pn[r] = cz<C>();
+        }
+        const R xn2 = block_sum<NT>(part, red);
+        // (2) reflector of step c-1: alpha = A'[c-1][c], x = A'[0..c-2][c]
+        R beta;
+        C tau, scal;
+        reflector(vn[c - 1], xn2, beta, tau, scal);
+        const bool act = !(tau.x == 0 && tau.y == 0);
+        __syncthreads();
+        if (tid == 0) dd[c] = vn[c].x;
+        for (int r = tid; r < c - 1; r += NT) {
+            const C x = act ? cmul(scal, vn[r]) : vn[r];
+            vn[r] = x;
+            *gs.at(r, c) = x;
+        }
+        if (tid == 0) {
+            vn[c - 1] = cm<C>(1, 0);
+            *gs.at(c - 1, c) = cm<C>(beta, 0);
+            ee[c - 1] = beta;
+            tt[c - 1] = tau;
+        }
+        __syncthreads();
+        // (3) pn = A v over the stored leading c x c block (read only)
+        fused_pass<NT>(gs, c, vn, vn, false, vn, act, pn);
+        // (4) w_q^H v (even slots) and v_q^H v (odd slots) for q < j
+        for (int t2 = warp; t2 < 2 * j; t2 += NW) {
+            const int q = t2 >> 1;
+            const C* y = (t2 & 1) ? V + (size_t)q * n : W + (size_t)q * n;
+            C sd = cz<C>();
+            for (int r = lane; r < c; r += 32) cfmac(sd, y[r], vn[r]);
+            sd = warp_sum(sd);
+            if (lane == 0) coef[t2] = sd;
+        }
+        __syncthreads();
+        // (5) x = tau (pn - sum_q V_q (w_q^H v) + W_q (v_q^H v)); w = x - tau/2 (x^H v) v
+        C dpart = cz<C>();
+        for (int r = tid; r < c; r += NT) {
+            C x = pn[r];
+            for (int q = 0; q < j; ++q) {
+                C u = cmul(V[(size_t)q * n + r], coef[2 * q]);
+                cfma(u, W[(size_t)q * n + r], coef[2 * q + 1]);
+                x = csub(x, u);
+            }
+            x = cmul(tau, x);
+            pn[r] = x;
+            cfmac(dpart, x, vn[r]);
+        }
+        const C xv = block_sum_c<NT>(dpart, red);
+        const C al = cscale(cmul(tau, xv), (R)-0.5);
+        C* vj = V + (size_t)j * n;
+        C* wj = W + (size_t)j * n;
+        for (int r = tid; r < c; r += NT) {
+            vj[r] = vn[r];
+            wj[r] = act ? cadd(pn[r], cmul(al, vn[r])) : cz<C>();
+        }
+        __syncthreads();
+    }
+}
+
+// [V | W] (r, k) and [W | V]^H (k, c) of a panel: the operands of A -= V W^H + W V^H.
+template <class C>
+struct OpPanelA {
+    static constexpr bool RFAST = true;
+    const C* pv;
+    const C* pw;
+    int n;
+    __device__ __forceinline__ C elem(size_t mat, int r, int k) const {
+        const size_t o = mat * (size_t)HP_W * n;
+        return k < HP_W ? pv[o + (size_t)k * n + r] : pw[o + (size_t)(k - HP_W) * n + r];
+    }
+};
+template <class C>
+struct OpPanelB {
+    static constexpr bool KFAST = false;
+    const C* pv;
+    const C* pw;
+    int n;
+    __device__ __forceinline__ C elem(size_t mat, int k, int c) const {
+        const size_t o = mat * (size_t)HP_W * n;
+        return cconj(k < HP_W ? pw[o + (size_t)k * n + c] : pv[o + (size_t)(k - HP_W) * n + c]);
+    }
+};
+// A(r, c) -= acc on and above the diagonal (real diagonal); tiles below it are skipped.
+template <class C>
+struct EpHer2k {
+    C* a;
+    int n;
+    __device__ __forceinline__ bool skip(int r0, int c0, int) const { return r0 > c0 + ZG_BN - 1; }
+    __device__ __forceinline__ void store(size_t mat, int r, int c, C acc) const {
+        if (r > c) return;
+        C* q = a + mat * (size_t)n * n + (size_t)c * n + r;
+        C x = csub(*q, acc);
+        if (r == c) x.y = 0;
+        *q = x;
     }
 };
 
@@ -1164,6 +1323,7 @@ struct EpResid {
     const double* w;
     cplx* res;
     int n;
+    __device__ __forceinline__ bool skip(int, int, int) const { return false; }
     __device__ __forceinline__ void store(size_t mat, int r, int c, cplx acc) const {
         const size_t o = mat * (size_t)n * n + (size_t)c * n + r;
         const cplx xr = to_c64(x[o]);
@@ -1250,6 +1410,7 @@ struct EpCoupling {
     const int2* cl;
     cplxf* f;
     int n;
+    __device__ __forceinline__ bool skip(int, int, int) const { return false; }
     __device__ __forceinline__ void store(size_t mat, int i, int j, cplx acc) const {
         cplxf val = make_float2(0.f, 0.f);
         if (i != j) {
@@ -1414,6 +1575,7 @@ struct EpUpdate {
     const XT* x;
     cplx* out;
     int n;
+    __device__ __forceinline__ bool skip(int, int, int) const { return false; }
     __device__ __forceinline__ void store(size_t mat, int r, int c, cplxf acc) const {
         const size_t o = mat * (size_t)n * n + (size_t)c * n + r;
         const cplx xr = to_c64(x[o]);
@@ -1478,16 +1640,16 @@ static HetrdCfg hetrd_config(int n) {
 }
 template <class R>
 static cudaError_t launch_hetrd(const HetrdCfg& c, cudaStream_t st, int nb, typename Cx<R>::T* A, double* D,
-                                double* E, typename Cx<R>::T* TAU, int n) {
+                                double* E, typename Cx<R>::T* TAU, int n, int m) {
     if (c.smem > 227 * 1024) return cudaErrorInvalidValue;
     if (c.nt == 128) {
         cudaError_t e = cudaFuncSetAttribute(k_hetrd<128, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
         if (e != cudaSuccess) return e;
-        k_hetrd<128, R><<<nb, 128, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
+        k_hetrd<128, R><<<nb, 128, c.smem, st>>>(A, D, E, TAU, n, m, c.tri_cap);
     } else {
         cudaError_t e = cudaFuncSetAttribute(k_hetrd<512, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
         if (e != cudaSuccess) return e;
-        k_hetrd<512, R><<<nb, 512, c.smem, st>>>(A, D, E, TAU, n, c.tri_cap);
+        k_hetrd<512, R><<<nb, 512, c.smem, st>>>(A, D, E, TAU, n, m, c.tri_cap);
     }
     return cudaGetLastError();
 }
@@ -1505,8 +1667,9 @@ struct HeevPlan {
     int ch, dbuf;
     size_t smem_orm;
     int nblk16, nblk64;
+    int npanels, m_tail;  // blocked reduction: panels of HP_W columns, then k_hetrd on m_tail
     size_t off_d, off_e, off_tau, off_a, off_z, off_lu, off_x, off_t, off_w, off_res, off_x1, off_cl,
-        off_y, off_mu, off_st, per;
+        off_y, off_mu, off_st, off_pv, per;
 };
 
 static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
@@ -1515,7 +1678,9 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     p.mixed = mixed;
     p.refine_steps = mixed ? refine_steps : 0;
     const size_t ce = mixed ? sizeof(cplxf) : sizeof(cplx);   // working complex element
-    p.hc = mixed ? hetrd_config<float>(n) : hetrd_config<double>(n);
+    p.npanels = n >= HT_BLOCKED_MIN ? (n - HT_TAIL + HP_W - 1) / HP_W : 0;
+    p.m_tail = n - p.npanels * HP_W;
+    p.hc = mixed ? hetrd_config<float>(p.m_tail) : hetrd_config<double>(p.m_tail);
     p.smem_tri = 4 * (size_t)n * sizeof(double) + n * sizeof(int);
     p.nblk16 = (n - 1 + ORM_NB - 1) / ORM_NB;
     p.nblk64 = (n - 1 + BT_NB - 1) / BT_NB;
@@ -1546,6 +1711,7 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     p.off_y = off; off += mixed ? r256((size_t)n * RF_KMAX * sizeof(cplx)) : 0;
     p.off_mu = off; off += mixed ? r256(n * sizeof(double)) : 0;
     p.off_st = off; off += mixed ? r256(3 * (size_t)n * sizeof(double)) : 0;
+    p.off_pv = off; off += p.npanels > 0 ? r256(2 * (size_t)HP_W * n * ce) : 0;   // panel V, W
     p.per = off;
     return p;
 }
@@ -1567,6 +1733,40 @@ size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n, false).per; }
     do {                      \
         if (ctx) prof_begin(ctx, name); \
     } while (0)
+
+// Householder tridiagonalisation in the working precision R: blocked panels (k_hetrd_panel +
+// rank-2*HP_W GEMM update) down to order m_tail, then k_hetrd on the leading block.  PV holds
+// the panel pairs of the chunk (V of every matrix, then W of every matrix).
+template <class R>
+static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, int nb, typename Cx<R>::T* A,
+                          double* D, double* E, typename Cx<R>::T* TAU, typename Cx<R>::T* PV,
+                          long long* launches) {
+    typedef typename Cx<R>::T C;
+    const int n = p.n;
+    int m = n;
+    if (p.npanels > 0) {
+        C* PWb = PV + (size_t)nb * HP_W * n;
+        const size_t smem = (2 * (size_t)n + 2 * HP_W) * sizeof(C) + 2 * (512 / 32) * sizeof(R);
+        if (cudaFuncSetAttribute(k_hetrd_panel<512, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return RLMB_ERR_CUDA;
+        for (int k = 0; k < p.npanels; ++k) {
+            RLMB_CHUNK_PROF("k_hetrd");
+            k_hetrd_panel<512, R><<<nb, 512, smem, st>>>(A, D, E, TAU, PV, PWb, n, m);
+            RLMB_CHUNK_LAUNCHED();
+            m -= HP_W;
+            RLMB_CHUNK_PROF("k_hetrd");
+            if (launch_zgemm<C, 64>(st, OpPanelA<C>{PV, PWb, n}, OpPanelB<C>{PV, PWb, n}, EpHer2k<C>{A, n}, m, m,
+                                    2 * HP_W, nb) != cudaSuccess)
+                return RLMB_ERR_CUDA;
+            RLMB_CHUNK_LAUNCHED();
+        }
+    }
+    RLMB_CHUNK_PROF("k_hetrd");
+    if (launch_hetrd<R>(p.hc, st, nb, A, D, E, TAU, n, m) != cudaSuccess) return RLMB_ERR_CUDA;
+    RLMB_CHUNK_LAUNCHED();
+    return RLMB_OK;
+}
 
 // Back-transformation X = Q Z in the working precision R (X column-major, column =
 // eigenvector): k_larft + k_ormtr, or for large orders k_larft64 + k_bt_w / k_bt_upd.
@@ -1693,9 +1893,9 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
         cplx* Xw = reinterpret_cast<cplx*>(base + p.off_x * B);
         cplx* Tw = reinterpret_cast<cplx*>(base + p.off_t * B);
         cplx* Wp = reinterpret_cast<cplx*>(base + p.off_w * B);
-        RLMB_CHUNK_PROF("k_hetrd");
-        if (launch_hetrd<double>(p.hc, st, nb, A, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
-        RLMB_CHUNK_LAUNCHED();
+        if (int rc = tridiagonalise<double>(ctx, st, p, nb, A, Dw, Ew, TAUw,
+                                            reinterpret_cast<cplx*>(base + p.off_pv * B), launches))
+            return rc;
         RLMB_CHUNK_PROF("k_stebz");
         k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
         RLMB_CHUNK_LAUNCHED();
@@ -1724,9 +1924,9 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     RLMB_CHUNK_PROF("k_to_single");
     k_to_single<<<2048, 256, 0, st>>>(A, As, B * nn);
     RLMB_CHUNK_LAUNCHED();
-    RLMB_CHUNK_PROF("k_hetrd");
-    if (launch_hetrd<float>(p.hc, st, nb, As, Dw, Ew, TAUw, n) != cudaSuccess) return RLMB_ERR_CUDA;
-    RLMB_CHUNK_LAUNCHED();
+    if (int rc = tridiagonalise<float>(ctx, st, p, nb, As, Dw, Ew, TAUw,
+                                       reinterpret_cast<cplxf*>(base + p.off_pv * B), launches))
+        return rc;
     RLMB_CHUNK_PROF("k_stebz");
     k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
     RLMB_CHUNK_LAUNCHED();

@@ -12,7 +12,8 @@
 //   A: la.elem(mat, r, k), LA::RFAST (r contiguous in memory, else k contiguous)
 //   B: lb.elem(mat, k, c), LB::KFAST (k contiguous in memory, else c contiguous)
 // called only inside the matrix (r < M, k < K, c < N); the epilogue ep.store(mat, r, c,
-// acc) is called once per output entry.
+// acc) is called once per output entry, and ep.skip(r0, c0, BM) may drop whole output tiles
+// (a triangular update).
 #pragma once
 #include "common.cuh"
 
@@ -38,6 +39,7 @@ k_zgemm(LA la, LB lb, EP ep, int M, int N, int K) {
     const int t = threadIdx.x, tr = t / 16, tc = t % 16;
     const size_t mat = blockIdx.z;
     const int r0 = blockIdx.x * BM, c0 = blockIdx.y * ZG_BN;
+    if (ep.skip(r0, c0, BM)) return;   // output tile not needed (whole CTA leaves together)
     C fa[EA], fb[EB];
     auto a_pos = [&](int e, int& kk, int& rr) {
         const int idx = t + 256 * e;
