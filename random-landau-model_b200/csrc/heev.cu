@@ -1150,6 +1150,79 @@ static constexpr int HP_W = 32;      // panel width
 static constexpr int HT_TAIL = 256;  // order below which the unblocked kernel finishes
 static constexpr int HT_BLOCKED_MIN = 640;   // orders from which the blocked reduction runs
 
+// p += A v for the Hermitian leading m x m block stored in the upper triangle of a
+// (column-major, leading dimension ld; read only), v and p in shared memory.  Work is dealt
+// to warps as strips of HV_W columns; a lane holds one row of a 32-row block of the strip:
+// its row contributions go to p[r] (shared atomics, once per block), its column
+// contributions conj(A[r][c]) v[r] stay in registers for the whole strip and are reduced
+// across the warp once at the end.  Interior blocks (entirely above the diagonal and inside
+// the matrix) run without predicates.
+static constexpr int HV_W = 8;
+template <int NT, class C>
+__device__ __forceinline__ void hemv_upper(const C* __restrict__ a, int ld, int m, const C* __restrict__ v,
+                                           C* p) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    const int nstrips = (m + HV_W - 1) / HV_W;
+    for (int s = warp; s < nstrips; s += NW) {
+        const int c0 = s * HV_W;
+        C vc[HV_W], e[HV_W];
+#pragma unroll
+        for (int j = 0; j < HV_W; ++j) {
+            vc[j] = c0 + j < m ? v[c0 + j] : cz<C>();
+            e[j] = cz<C>();
+        }
+        const C* colp = a + (size_t)c0 * ld;
+        const int rend = min(c0 + HV_W, m);   // rows that meet the strip on or above the diagonal
+        const bool full = c0 + HV_W <= m;
+#pragma unroll 1
+        for (int r0 = 0; r0 < rend; r0 += 32) {
+            const int r = r0 + lane;
+            const bool interior = full && r0 + 32 <= c0;
+            C x[HV_W];
+            if (interior) {
+#pragma unroll
+                for (int j = 0; j < HV_W; ++j) x[j] = colp[(size_t)j * ld + r];
+            } else {
+#pragma unroll
+                for (int j = 0; j < HV_W; ++j) {
+                    const int cc = c0 + j;
+                    x[j] = (cc < m && r <= cc) ? colp[(size_t)j * ld + r] : cz<C>();
+                }
+            }
+            const C vr = r < m ? v[r] : cz<C>();
+            C rowacc = cz<C>();
+#pragma unroll
+            for (int j = 0; j < HV_W; ++j) {
+                if (interior || r < c0 + j) {
+                    cfma(rowacc, x[j], vc[j]);
+                    cfmac(e[j], x[j], vr);
+                } else if (r == c0 + j) {
+                    rowacc = cadd(rowacc, cscale(vc[j], x[j].x));
+                }
+            }
+            if (r < rend) smem_atomic_add(&p[r], rowacc);
+        }
+        // column sums: lane l ends with the sum over the warp of e[l & 7]
+#pragma unroll
+        for (int j = 0; j < HV_W; ++j) {
+            e[j] = cadd(e[j], shfl_xor(e[j], 16));
+            e[j] = cadd(e[j], shfl_xor(e[j], 8));
+        }
+#pragma unroll
+        for (int sh = 4; sh >= 1; sh >>= 1) {
+            const bool up = (lane & sh) != 0;
+#pragma unroll
+            for (int j = 0; j < sh; ++j) {
+                const C send = up ? e[j] : e[j + sh];
+                const C keep = up ? e[j + sh] : e[j];
+                e[j] = cadd(keep, shfl_xor(send, sh));
+            }
+        }
+        if (lane < HV_W && c0 + lane < m) smem_atomic_add(&p[c0 + lane], e[0]);
+    }
+}
+
 template <int NT, class R>
 __global__ void __launch_bounds__(NT, 1)
 k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
@@ -1213,7 +1286,7 @@ k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double*
         }
         __syncthreads();
         // (3) pn = A v over the stored leading c x c block (read only)
-        fused_pass<NT>(gs, c, vn, vn, false, vn, act, pn);
+        if (act) hemv_upper<NT>(gs.a, n, c, vn, pn);
         // (4) w_q^H v (even slots) and v_q^H v (odd slots) for q < j
         for (int t2 = warp; t2 < 2 * j; t2 += NW) {
             const int q = t2 >> 1;
