@@ -1147,8 +1147,8 @@ struct EpSub {     // X(r, c) -= acc
 // over all SMs (k_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
 // k_hetrd.  D, E, TAU and the reflector storage are those of the unblocked reduction.
 static constexpr int HP_W = 32;      // panel width
-static constexpr int HT_TAIL = 256;  // order below which the unblocked kernel finishes
-static constexpr int HT_BLOCKED_MIN = 640;   // orders from which the blocked reduction runs
+static constexpr int HT_TAIL = 128;  // order below which the unblocked kernel finishes
+static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
 
 // p += A v for the Hermitian leading m x m block stored in the upper triangle of a
 // (column-major, leading dimension ld; read only), v and p in shared memory.  Work is dealt
