@@ -962,53 +962,43 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
 // global memory (column-major, column = eigenvector) and is read twice and written once
 // per block.
 static constexpr int BT_NB = 64;
+static constexpr int BT_GEMM_MIN = 384;   // order from which the GEMM back-transformation runs
 
-// T factor of block j (reflectors 64j .. 64j+63) of one matrix; grid (blocks, matrices).
+// T factor of block j (reflectors 64j .. 64j+63) of one matrix from its Gram matrix
+// G = V_j^H V_j (column-major 64 x 64, computed by a batched GEMM into the same slot of Tw):
+//   T[k][k] = tau_k,  T[k][q] = -tau_k sum_{l=q}^{k-1} G[k][l] T[l][q]   (q < k),
+// written back row-major (T[k][q] at k*64 + q); grid (blocks, matrices), 64 threads.
 template <class R>
-__global__ void __launch_bounds__(256)
-k_larft64(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __restrict__ TAU,
-          typename Cx<R>::T* __restrict__ Tw, int n) {
+__global__ void __launch_bounds__(64)
+k_larft64(const typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ Tw, int n) {
     typedef typename Cx<R>::T C;
+    typedef C Row[BT_NB + 1];
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* G = reinterpret_cast<C*>(smem_raw);   // [64][64]
-    C* T = G + BT_NB * BT_NB;                   // [64][64]
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int j = blockIdx.x;
+    Row* G = reinterpret_cast<Row*>(smem_raw);   // G[l][k] = v_k^H v_l (column l of the Gram matrix)
+    Row* T = G + BT_NB;
+    const int j = blockIdx.x, q = threadIdx.x;
     const size_t mat = blockIdx.y;
-    const C* a = A + mat * (size_t)n * n;
     const C* tau = TAU + mat * n;
     const int nblk = (n - 1 + BT_NB - 1) / BT_NB;
     const int i0 = j * BT_NB;
-    for (int pr = warp; pr < BT_NB * BT_NB; pr += 8) {
-        const int k = pr / BT_NB, l = pr % BT_NB;
-        if (l >= k) continue;
-        const int ik = i0 + k, il = i0 + l;
-        C s = cz<C>();
-        if (ik <= n - 2)
-            for (int r = lane; r <= il; r += 32) cfmac(s, refl_entry(a, n, ik, r), refl_entry(a, n, il, r));
-        s = warp_sum(s);
-        if (lane == 0) G[k * BT_NB + l] = s;
-    }
+    C* blk = Tw + (mat * nblk + j) * BT_NB * BT_NB;
+    for (int l = 0; l < BT_NB; ++l) G[l][q] = blk[l * BT_NB + q];
     __syncthreads();
     for (int k = 0; k < BT_NB; ++k) {
         const int ik = i0 + k;
         const C tk = ik <= n - 2 ? tau[ik] : cz<C>();
-        if (threadIdx.x < BT_NB) {
-            const int q = threadIdx.x;
-            C val = cz<C>();
-            if (q == k) {
-                val = tk;
-            } else if (q < k) {
-                C s = cz<C>();
-                for (int l = q; l < k; ++l) cfma(s, G[k * BT_NB + l], T[l * BT_NB + q]);
-                val = cscale(cmul(tk, s), (R)-1);
-            }
-            T[k * BT_NB + q] = val;
+        C val = cz<C>();
+        if (q == k) {
+            val = tk;
+        } else if (q < k) {
+            C sum = cz<C>();
+            for (int l = q; l < k; ++l) cfma(sum, G[l][k], T[l][q]);
+            val = cscale(cmul(tk, sum), (R)-1);
         }
+        T[k][q] = val;
         __syncthreads();
     }
-    C* out = Tw + (mat * nblk + j) * BT_NB * BT_NB;
-    for (int i = threadIdx.x; i < BT_NB * BT_NB; i += 256) out[i] = T[i];
+    for (int k = 0; k < BT_NB; ++k) blk[k * BT_NB + q] = T[k][q];
 }
 
 // Z (row-major real) -> X (column-major complex), grid-stride over all batch entries.
@@ -1085,6 +1075,29 @@ struct OpReflH {
         C v = refl_entry(a + mat * (size_t)n * n, n, i0 + q, r);
         v.y = -v.y;
         return v;
+    }
+};
+
+// Gram matrices of all 64-reflector blocks in one batched GEMM: batch index z = mat * nblk
+// + j; A(q, r) = conj(v_{64j+q}[r]), B(r, l) = v_{64j+l}[r].
+template <class C>
+struct OpBlkReflH {
+    static constexpr bool RFAST = false;
+    const C* a;
+    int n, nblk;
+    __device__ __forceinline__ C elem(size_t z, int q, int r) const {
+        C v = refl_entry(a + (z / nblk) * (size_t)n * n, n, (int)(z % nblk) * BT_NB + q, r);
+        v.y = -v.y;
+        return v;
+    }
+};
+template <class C>
+struct OpBlkRefl {
+    static constexpr bool KFAST = true;
+    const C* a;
+    int n, nblk;
+    __device__ __forceinline__ C elem(size_t z, int r, int l) const {
+        return refl_entry(a + (z / nblk) * (size_t)n * n, n, (int)(z % nblk) * BT_NB + l, r);
     }
 };
 
@@ -1765,7 +1778,9 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     if (!p.dbuf)
         smem = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * ce;
     p.smem_orm = smem;
-    p.small_bt = (n + 256 / ch - 1) / (256 / ch) <= ORM_RPT && smem <= 220 * 1024;
+    // register-resident k_ormtr up to order 383 (it fits and beats the GEMM path there), the
+    // GEMM path from 384 on
+    p.small_bt = n < BT_GEMM_MIN && (n + 256 / ch - 1) / (256 / ch) <= ORM_RPT && smem <= 220 * 1024;
     const size_t nn = (size_t)n * n;
     auto r256 = [](size_t v) { return (v + 255) / 256 * 256; };
     size_t off = 0;
@@ -1842,7 +1857,8 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
 }
 
 // Back-transformation X = Q Z in the working precision R (X column-major, column =
-// eigenvector): k_larft + k_ormtr, or for large orders k_larft64 + k_bt_w / k_bt_upd.
+// eigenvector): k_larft + k_ormtr, or the blocked GEMM path (Gram GEMM + k_larft64, then
+// three GEMMs per block of 64 reflectors).
 template <class R>
 static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, int nb,
                           const typename Cx<R>::T* Aw, const typename Cx<R>::T* TAUw, const double* Zw,
@@ -1866,11 +1882,16 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         RLMB_CHUNK_LAUNCHED();
         return RLMB_OK;
     }
-    const size_t smem_t = 2 * BT_NB * BT_NB * sizeof(C);
+    RLMB_CHUNK_PROF("k_larft");
+    if (launch_zgemm<C, 64>(st, OpBlkReflH<C>{Aw, n, p.nblk64}, OpBlkRefl<C>{Aw, n, p.nblk64},
+                            EpStore<C>{Tw, BT_NB, (size_t)BT_NB * BT_NB}, BT_NB, BT_NB, n, nb * p.nblk64) != cudaSuccess)
+        return RLMB_ERR_CUDA;
+    RLMB_CHUNK_LAUNCHED();
+    const size_t smem_t = 2 * BT_NB * (BT_NB + 1) * sizeof(C);
     if (cudaFuncSetAttribute(k_larft64<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_PROF("k_larft");
-    k_larft64<R><<<dim3(p.nblk64, nb), 256, smem_t, st>>>(Aw, TAUw, Tw, n);
+    k_larft64<R><<<dim3(p.nblk64, nb), BT_NB, smem_t, st>>>(TAUw, Tw, n);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ormtr");
     k_z_to_x<C><<<2048, 256, 0, st>>>(Zw, Xw, n, (size_t)nb * nn);
@@ -2048,6 +2069,7 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     budget = std::max<size_t>(budget, per);
     size_t chunk = std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)batch));
     chunk = std::min<size_t>(chunk, 65535);   // grid y / z extent of the per-matrix launches
+    if (!plan.small_bt) chunk = std::min<size_t>(chunk, 65535 / std::max(plan.nblk64, 1));   // (matrix, block) batches
     if (int rc = ensure_workspace(ctx, chunk * per)) return rc;
     const size_t nn = (size_t)n * n;
     long long unused = 0;
