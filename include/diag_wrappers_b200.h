@@ -55,4 +55,9 @@ void generate_disorder_potential(double* impurity_x, double* impurity_y, double*
                                  int impurity_num, double L1, double L2, unsigned long seed,
                                  int sample_offset);
 
+/* diag_wrappers/wfs_file.h:11-12 -- raw eigenvector files wfs_<theta_1>_<theta_2>.bin in the
+ * current directory, size complex values (host). */
+void write_wfs(int theta_1, int theta_2, std::complex<double>* wfs, unsigned long size);
+void read_wfs(int theta_1, int theta_2, std::complex<double>* wfs, unsigned long size);
+
 #endif

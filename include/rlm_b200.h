@@ -106,6 +106,12 @@ int rlmb_rlm_coeff_tables(int n_phi, int off_head, int dim, int n_mesh, double L
 /* Impurities of one sample, as rlm/disorder_potential.cpp:3-21 draws them (host MT19937). */
 int rlmb_rlm_disorder(int impurity_num, double L1, double L2, unsigned long seed, int sample,
                       double* h_x, double* h_y, double* h_s);
+/* The same draws on the device, for samples sample0 .. sample0+count-1 at once (one
+ * MT19937 stream per sample, skipped on the device): d_x, d_y, d_s are count*impurity_num
+ * doubles, sample k at [k*impurity_num], bit-identical to rlmb_rlm_disorder. */
+int rlmb_rlm_disorder_device(rlmb_context* ctx, int impurity_num, double L1, double L2,
+                             unsigned long seed, int sample0, int count, double* d_x, double* d_y,
+                             double* d_s);
 /* V_mn of one or more samples (rlm/matrix_coefficients.cpp:27-44, rlm/potential_coeff.cu:3-26):
  * d_x,d_y,d_s: n_samples*impurity_num; d_vmn: n_samples*dim*dim complex, row-major m*dim+n. */
 int rlmb_rlm_potential(rlmb_context* ctx, const double* d_x, const double* d_y, const double* d_s,
@@ -123,6 +129,11 @@ int rlmb_rlm_assemble(rlmb_context* ctx, const double* d_vmn, const double* d_co
  * On-site potentials of n_sample samples from one run-long stream
  * (hlm/main_hlm_cpu.cpp:345-358): h_out[n_sample*n_sites]. */
 int rlmb_hlm_potentials(unsigned long seed, int n_sites, int n_sample, double* h_out);
+/* hlm potentials of samples sample0 .. sample0+count-1 drawn on the device (outputs
+ * [sample*n_sites, (sample+1)*n_sites) of the run's single stream), bit-identical to
+ * rlmb_hlm_potentials; d_out is count*n_sites doubles. */
+int rlmb_hlm_potentials_device(rlmb_context* ctx, unsigned long seed, int n_sites, int sample0,
+                               int count, double* d_out);
 /* Clean Bloch basis W(theta_1,theta_2) of band `band` (hlm/hamiltonian_hlm_cpu.cpp:2-56):
  * d_wfs receives n_sites*n_phi complex, column-major (column kx*ly+ky). */
 int rlmb_hlm_basis(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh, int theta_1,
@@ -148,6 +159,16 @@ int rlmb_fhs_line(rlmb_context* ctx, const double* d_prev, const double* d_cur, 
 int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double quanta_concentration,
                         double impurity_concentration, int n_mesh, unsigned long seed,
                         int sample0, int n_samples, double* h_energies, double* h_chern);
+/* rlm, one sample, with its eigenvectors exported: besides the energies and Chern numbers
+ * of rlmb_rlm_mesh_solve, every k-point's eigenvector matrix is written to
+ * dir/wfs_<theta_1>_<theta_2>.bin (theta_1, theta_2 in 0..n_mesh) in the raw format of the
+ * reference's write_wfs (diag_wrappers/wfs_file.cpp:2-11; rlm/main_rlm_gpu.cu:187,227 with
+ * -DwfsIO): n_phi*n_phi complex doubles, column k = eigenvector k.  The reference keeps only
+ * two theta_1 lines (file names use theta_1 % 2); here every line is kept.  Eigenvector
+ * phases are those of this solver (any phase is an eigenvector; FHS is gauge invariant). */
+int rlmb_rlm_mesh_export(rlmb_context* ctx, int n_phi, double quanta_concentration,
+                         double impurity_concentration, int n_mesh, unsigned long seed, int sample,
+                         const char* dir, double* h_energies, double* h_chern);
 /* hlm: n_samples samples with the given potentials (hlm/main_hlm_cpu.cpp:354-475). */
 int rlmb_hlm_mesh_solve(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh,
                         const double* h_potentials, int n_samples, double* h_energies,

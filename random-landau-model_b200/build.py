@@ -22,8 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + INCLUDE]
 
-CU_SOURCES = ["heev.cu", "model_kernels.cu", "capi.cu", "profile.cu", "heev_noalloc.cu", "diag_wrappers.cu"]
-DRIVERS = {"rlm": "tools/rlm_main.cpp", "hlm": "tools/hlm_main.cpp"}
+CU_SOURCES = ["heev.cu", "model_kernels.cu", "capi.cu", "profile.cu", "heev_noalloc.cu", "diag_wrappers.cu", "disorder.cu"]
+DRIVERS = {"rlm": "tools/rlm_main.cpp", "hlm": "tools/hlm_main.cpp", "rlm_fss": "tools/rlm_fss_main.cpp"}
 CPP_SOURCES = ["host_tables.cpp"]
 
 

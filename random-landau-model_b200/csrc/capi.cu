@@ -310,9 +310,77 @@ int rlmb_fhs_line(rlmb_context* ctx, const double* d_prev, const double* d_cur, 
 }
 
 // --------------------------------------------------------------------- rlm pipeline
+// Eigenvector matrices of one sample's mesh, already solved in place in d_H (kpts matrices
+// of n x n complex128), written as wfs_<t1>_<t2>.bin under dir: the raw layout of the
+// reference's write_wfs (diag_wrappers/wfs_file.cpp:2-11, dim_wfs complex values, column k
+// = eigenvector k).  Device-to-host copies go through two pinned slots on the context
+// stream, so that the copy of k-point t overlaps the file write of k-point t-1.
+static int export_wfs(rlmb_context* ctx, const cplx* d_H, int n, int g, const char* dir) {
+    const size_t nn = (size_t)n * n, bytes = nn * sizeof(cplx);
+    const int kpts = (g + 1) * (g + 1);
+    if (int rc = ensure_pinned(ctx, 2 * bytes)) return rc;
+    unsigned char* slot[2] = {static_cast<unsigned char*>(ctx->pinned),
+                              static_cast<unsigned char*>(ctx->pinned) + bytes};
+    cudaEvent_t ev[2];
+    RLMB_CUDA_TRY(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    if (cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        return RLMB_ERR_CUDA;
+    }
+    int rc = RLMB_OK;
+    auto write = [&](int t) -> int {
+        char name[4096];
+        snprintf(name, sizeof(name), "%s/wfs_%d_%d.bin", dir, t / (g + 1), t % (g + 1));
+        FILE* f = fopen(name, "wb");
+        if (!f) {
+            fprintf(stderr, "rlmb: cannot write %s\n", name);
+            return RLMB_ERR_ARG;
+        }
+        const size_t w = fwrite(slot[t & 1], 1, bytes, f);
+        fclose(f);
+        return w == bytes ? RLMB_OK : RLMB_ERR_ARG;
+    };
+    for (int t = 0; t <= kpts && rc == RLMB_OK; ++t) {
+        if (t < kpts) {
+            if (cudaMemcpyAsync(slot[t & 1], d_H + (size_t)t * nn, bytes, cudaMemcpyDeviceToHost, ctx->stream) !=
+                    cudaSuccess ||
+                cudaEventRecord(ev[t & 1], ctx->stream) != cudaSuccess) {
+                rc = RLMB_ERR_CUDA;
+                break;
+            }
+        }
+        if (t > 0) {
+            if (cudaEventSynchronize(ev[(t - 1) & 1]) != cudaSuccess) {
+                rc = RLMB_ERR_CUDA;
+                break;
+            }
+            rc = write(t - 1);
+        }
+    }
+    if (rc != RLMB_OK) cudaStreamSynchronize(ctx->stream);   // no copy left in flight into the slots
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return rc;
+}
+
+static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh, unsigned long seed,
+                    int sample0, int n_samples, double* h_energies, double* h_chern, const char* wfs_dir);
+
 int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh,
                         unsigned long seed, int sample0, int n_samples, double* h_energies,
                         double* h_chern) {
+    return rlm_mesh(ctx, n_phi, qc, ic, n_mesh, seed, sample0, n_samples, h_energies, h_chern, nullptr);
+}
+
+int rlmb_rlm_mesh_export(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh,
+                         unsigned long seed, int sample, const char* dir, double* h_energies,
+                         double* h_chern) {
+    if (!dir) return RLMB_ERR_ARG;
+    return rlm_mesh(ctx, n_phi, qc, ic, n_mesh, seed, sample, 1, h_energies, h_chern, dir);
+}
+
+static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh, unsigned long seed,
+                    int sample0, int n_samples, double* h_energies, double* h_chern, const char* wfs_dir) {
     if (!ctx || n_phi <= 0 || !(qc > 0) || !(ic > 0) || n_mesh <= 0 || sample0 < 0 || n_samples < 0 ||
         (n_samples > 0 && (!h_energies || !h_chern)))
         return RLMB_ERR_ARG;
@@ -376,17 +444,10 @@ int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int 
     }
     for (int s0 = 0; s0 < n_samples; s0 += nb) {
         const int cnt = std::min(nb, n_samples - s0);
-        double* px = static_cast<double*>(ctx->pinned);
-        for (int s = 0; s < cnt; ++s) {
-            double* base = px + 3 * (size_t)nimp * s;
-            if (int rc = rlmb_rlm_disorder(nimp, L1, L2, seed, sample0 + s0 + s, base, base + nimp, base + 2 * (size_t)nimp))
-                return rc;
-        }
-        // reorder [sample][x|y|s] into three [sample][i] arrays on the device
-        for (int s = 0; s < cnt; ++s)
-            for (int c = 0; c < 3; ++c)
-                RLMB_CUDA_TRY(cudaMemcpyAsync(d_imp + ((size_t)c * nb + s) * nimp, px + (3 * (size_t)s + c) * nimp,
-                                              nimp * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        // disorder drawn on the device, bit-identical to the host stream (csrc/disorder.cu)
+        if (int rc = rlmb_rlm_disorder_device(ctx, nimp, L1, L2, seed, sample0 + s0, cnt, d_imp,
+                                              d_imp + (size_t)nb * nimp, d_imp + 2 * (size_t)nb * nimp))
+            return rc;
         if (int rc = ensure_workspace(ctx, rlm_potential_ws_elems(nimp, cnt, dim) * sizeof(cplx))) return rc;
         if (int rc = launch_rlm_potential(ctx, d_imp, d_imp + (size_t)nb * nimp, d_imp + 2 * (size_t)nb * nimp,
                                           nimp, cnt, d_cmn, dim, o, static_cast<cplx*>(ctx->ws), d_vmn))
@@ -397,6 +458,8 @@ int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int 
         if (int rc = rlmb_heevd_batched(ctx, reinterpret_cast<double*>(d_H), d_W, n_phi, cnt * kpts, d_info))
             return rc;
         if (int rc = count_failures(ctx, d_info, cnt * kpts, &failures)) return rc;
+        if (wfs_dir)
+            if (int rc = export_wfs(ctx, d_H, n_phi, g, wfs_dir)) return rc;   // one sample (cnt == 1)
         cplx* d_U1 = d_U;
         cplx* d_U2 = d_U + (size_t)n_phi * kpts * nb;
         if (int rc = launch_rlm_links(ctx, d_H, n_phi, g, cnt, d_U1, d_U2)) return rc;

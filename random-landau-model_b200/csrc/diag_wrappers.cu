@@ -193,3 +193,25 @@ void generate_disorder_potential(double* impurity_x, double* impurity_y, double*
     report("generate_disorder_potential",
            rlmb_rlm_disorder(impurity_num, L1, L2, seed, sample_offset, impurity_x, impurity_y, impurity_intensity));
 }
+
+// diag_wrappers/wfs_file.cpp:2-23: raw dumps named wfs_<theta_1>_<theta_2>.bin in the current
+// directory (no header, size complex doubles); a failure is reported on stderr.
+static void wfs_name(char* buf, size_t cap, int theta_1, int theta_2) {
+    snprintf(buf, cap, "wfs_%d_%d.bin", theta_1, theta_2);
+}
+
+void write_wfs(int theta_1, int theta_2, std::complex<double>* wfs, unsigned long size) {
+    char name[64];
+    wfs_name(name, sizeof(name), theta_1, theta_2);
+    FILE* f = fopen(name, "wb");
+    if (!f || fwrite(wfs, sizeof(std::complex<double>), size, f) != size) fprintf(stderr, "write_wfs: cannot write %s\n", name);
+    if (f) fclose(f);
+}
+
+void read_wfs(int theta_1, int theta_2, std::complex<double>* wfs, unsigned long size) {
+    char name[64];
+    wfs_name(name, sizeof(name), theta_1, theta_2);
+    FILE* f = fopen(name, "rb");
+    if (!f || fread(wfs, sizeof(std::complex<double>), size, f) != size) fprintf(stderr, "read_wfs: cannot read %s\n", name);
+    if (f) fclose(f);
+}

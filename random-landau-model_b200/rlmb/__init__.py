@@ -54,6 +54,11 @@ _SIGNATURES = {
     "rlmb_rlm_mesh_solve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_int, ctypes.c_ulong, ctypes.c_int, ctypes.c_int,
                                            _c_dp, _c_dp]),
+    "rlmb_rlm_mesh_export": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_ulong, ctypes.c_int, ctypes.c_char_p, _c_dp, _c_dp]),
+    "rlmb_rlm_disorder_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulong,
+                                                 ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "rlmb_hlm_potentials_device": (ctypes.c_int, [_vp, ctypes.c_ulong, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     "rlmb_hlm_mesh_solve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, _c_dp, ctypes.c_int, _c_dp, _c_dp]),
     "rlmb_hlm_mesh_solve_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -311,6 +316,37 @@ class Context:
                                        n_mesh, seed, sample0, n_samples, _dp(e), _dp(c))
         self.last_failures = max(rc, 0)
         _check(rc, "rlmb_rlm_mesh_solve")
+        return e, c
+
+    def rlm_disorder_device(self, impurity_num, L1, L2, seed, sample0, count):
+        """(x, y, s) torch float64 CUDA tensors [count, impurity_num] drawn on the device."""
+        import torch
+        out = [torch.empty((count, impurity_num), dtype=torch.float64, device="cuda") for _ in range(3)]
+        self.sync_stream()
+        _check(lib().rlmb_rlm_disorder_device(self.h, impurity_num, L1, L2, seed, sample0, count,
+                                              *[_ptr(t) for t in out]), "rlmb_rlm_disorder_device")
+        return out
+
+    def hlm_potentials_device(self, seed, n_sites, sample0, count):
+        """torch float64 CUDA tensor [count, n_sites] of hlm potentials drawn on the device."""
+        import torch
+        out = torch.empty((count, n_sites), dtype=torch.float64, device="cuda")
+        self.sync_stream()
+        _check(lib().rlmb_hlm_potentials_device(self.h, seed, n_sites, sample0, count, _ptr(out)),
+               "rlmb_hlm_potentials_device")
+        return out
+
+    def rlm_mesh_export(self, n_phi, quanta_concentration, impurity_concentration, n_mesh, seed, sample,
+                        directory):
+        """One sample of rlm_mesh_solve that also writes every k-point's eigenvectors to
+        directory/wfs_<theta_1>_<theta_2>.bin; returns (energies, chern) [n_phi]."""
+        e = np.zeros(n_phi)
+        c = np.zeros(n_phi)
+        self.sync_stream()
+        rc = lib().rlmb_rlm_mesh_export(self.h, n_phi, quanta_concentration, impurity_concentration, n_mesh,
+                                        seed, sample, os.fsencode(directory), _dp(e), _dp(c))
+        self.last_failures = max(rc, 0)
+        _check(rc, "rlmb_rlm_mesh_export")
         return e, c
 
     def hlm_mesh_solve(self, lx, ly, Q, band, n_mesh, potentials):

@@ -339,3 +339,24 @@ def test_rlm_large_order_matches_reference(ctx):
     assert np.abs(e[0] - eref).max() <= 1e-10 * np.abs(eref).max()
     assert np.array_equal(np.rint(c[0]), np.rint(cref))
     assert np.abs(c[0] - cref).max() < 1e-8
+
+
+# ------------------------------------------------------------- device disorder generation
+@pytest.mark.parametrize("nimp,samples", [(256, [0, 1, 5]), (8192, [0, 3, 31]), (48000, [0, 7])])
+def test_rlm_disorder_device_matches_host(ctx, nimp, samples):
+    """MT19937 on the device, skipped per sample, equals the host stream bit for bit."""
+    import rlmb
+    L = float(np.sqrt(nimp / 16.0))
+    lo, hi = min(samples), max(samples)
+    x, y, s = (t.cpu().numpy() for t in ctx.rlm_disorder_device(nimp, L, L, 1, lo, hi - lo + 1))
+    for smp in samples:
+        hx, hy, hs = rlmb.rlm_disorder(nimp, L, L, 1, smp)
+        k = smp - lo
+        assert np.array_equal(x[k], hx) and np.array_equal(y[k], hy) and np.array_equal(s[k], hs)
+
+
+def test_hlm_potentials_device_matches_host(ctx):
+    import rlmb
+    host = rlmb.hlm_potentials(1, 768, 70)
+    dev = ctx.hlm_potentials_device(1, 768, 3, 67).cpu().numpy()
+    assert np.array_equal(dev, host[3:70])
