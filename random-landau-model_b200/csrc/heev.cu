@@ -1160,7 +1160,7 @@ struct EpSub {     // X(r, c) -= acc
 // over all SMs (k_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
 // k_hetrd.  D, E, TAU and the reflector storage are those of the unblocked reduction.
 static constexpr int HP_W = 32;      // panel width
-static constexpr int HT_TAIL = 128;  // order below which the unblocked kernel finishes
+static constexpr int HT_TAIL = 96;   // order below which the unblocked kernel finishes
 static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
 
 // p += A v for the Hermitian leading m x m block stored in the upper triangle of a
@@ -1237,7 +1237,7 @@ __device__ __forceinline__ void hemv_upper(const C* __restrict__ a, int ld, int 
 }
 
 template <int NT, class R>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
 k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
               typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ PV,
               typename Cx<R>::T* __restrict__ PW, int n, int m) {
@@ -1834,13 +1834,16 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
     int m = n;
     if (p.npanels > 0) {
         C* PWb = PV + (size_t)nb * HP_W * n;
-        const size_t smem = (2 * (size_t)n + 2 * HP_W) * sizeof(C) + 2 * (512 / 32) * sizeof(R);
-        if (cudaFuncSetAttribute(k_hetrd_panel<512, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
+        // 256 threads (two CTAs per SM) for orders 385..512, 512 threads otherwise (measured)
+        const bool mid = n > 384 && n <= 512;
+        auto panel = mid ? k_hetrd_panel<256, R> : k_hetrd_panel<512, R>;
+        const int pnt = mid ? 256 : 512;
+        const size_t smem = (2 * (size_t)n + 2 * HP_W) * sizeof(C) + 2 * (pnt / 32) * sizeof(R);
+        if (cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return RLMB_ERR_CUDA;
         for (int k = 0; k < p.npanels; ++k) {
             RLMB_CHUNK_PROF("k_hetrd");
-            k_hetrd_panel<512, R><<<nb, 512, smem, st>>>(A, D, E, TAU, PV, PWb, n, m);
+            panel<<<nb, pnt, smem, st>>>(A, D, E, TAU, PV, PWb, n, m);
             RLMB_CHUNK_LAUNCHED();
             m -= HP_W;
             RLMB_CHUNK_PROF("k_hetrd");
