@@ -554,9 +554,31 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
     //      on det(T - x I) once the bracket holds k alone (dstebz bracketing, restated)
     if (PHASE == 1) {
     const double atol = 2.0 * DBL_EPSILON * onenrm;
+    // one collective pass first: Sturm counts at the TRI_THREADS+1 equally spaced points of
+    // the Gershgorin interval (count 0 at its left end, n at its right end), so that every
+    // eigenvalue starts from the grid cell holding it instead of the whole interval
+    __shared__ double s_gx[TRI_THREADS + 1];
+    __shared__ int s_gc[TRI_THREADS + 1];
+    {
+        const double gl = s_gl, gu = s_gu;
+        const int t = tid;
+        s_gx[t] = t == 0 ? gl : gl + (gu - gl) * ((double)t / TRI_THREADS);
+        if (t == 0) {
+            s_gc[0] = 0;
+            s_gx[TRI_THREADS] = gu;
+            s_gc[TRI_THREADS] = n;
+        } else {
+            double rr;
+            s_gc[t] = sturm_poly(d, e2, n, s_gx[t], pivmin, rr);
+        }
+    }
+    __syncthreads();
     for (int k = tid; k < n; k += TRI_THREADS) {
-        double lo = s_gl, hi = s_gu;
-        int clo = 0, chi = n;
+        int cell = 0;   // largest grid point with count <= k
+        for (int step = TRI_THREADS / 2; step >= 1; step >>= 1)
+            if (cell + step < TRI_THREADS && s_gc[cell + step] <= k) cell += step;
+        double lo = s_gx[cell], hi = s_gx[cell + 1];
+        int clo = s_gc[cell], chi = s_gc[cell + 1];
         double x = 0.5 * (lo + hi);
         double res = x;
         bool done = false;
