@@ -410,6 +410,45 @@ __device__ __forceinline__ int sturm_poly(const double* __restrict__ d, const do
     return cnt;
 }
 
+// The counts of sturm_poly at two shifts, the two recurrences interleaved (no derivatives).
+__device__ __forceinline__ void sturm_count2(const double* __restrict__ d, const double* __restrict__ e2, int n,
+                                             double xa, double xb, double pivmin, int& ca, int& cb) {
+    double pma = 1.0, pa = d[0] - xa, pmb = 1.0, pb = d[0] - xb;
+    if (fabs(pa) <= pivmin) pa = -pivmin;
+    if (fabs(pb) <= pivmin) pb = -pivmin;
+    int na = pa < 0.0, nb = pb < 0.0;
+    for (int j = 1; j < n; ++j) {
+        const double ee = e2[j - 1], dj = d[j];
+        double qa = fma(dj - xa, pa, -ee * pma);
+        double qb = fma(dj - xb, pb, -ee * pmb);
+        if (fabs(qa) <= pivmin * fabs(pa)) qa = -pivmin * pa;
+        if (fabs(qb) <= pivmin * fabs(pb)) qb = -pivmin * pb;
+        na += (qa < 0.0) != (pa < 0.0);
+        nb += (qb < 0.0) != (pb < 0.0);
+        pma = pa;
+        pa = qa;
+        pmb = pb;
+        pb = qb;
+        const double biga = fmax(fabs(pa), fabs(pma)), bigb = fmax(fabs(pb), fabs(pmb));
+        if (biga > 0x1p+400 || biga < 0x1p-400) {
+            int ex;
+            frexp(biga, &ex);
+            const double sc = ldexp(1.0, -ex);
+            pa *= sc;
+            pma *= sc;
+        }
+        if (bigb > 0x1p+400 || bigb < 0x1p-400) {
+            int ex;
+            frexp(bigb, &ex);
+            const double sc = ldexp(1.0, -ex);
+            pb *= sc;
+            pmb *= sc;
+        }
+    }
+    ca = na;
+    cb = nb;
+}
+
 // deterministic start vector entries in (-1, 1)
 __device__ __forceinline__ double start_entry(int k, int j) {
     uint32_t h = (uint32_t)k * 0x9E3779B1u ^ ((uint32_t)j * 0x85EBCA77u + 0x165667B1u);
@@ -595,9 +634,8 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
                     if (fabs(nt - x) <= tol) {
                         // converged step: accept only if Sturm counts bracket index k at nt +- 2 tol
                         const double a0 = fmax(lo, nt - 2.0 * tol), b0 = fmin(hi, nt + 2.0 * tol);
-                        double rr;
-                        const int ca = sturm_poly(d, e2, n, a0, pivmin, rr);
-                        const int cb = sturm_poly(d, e2, n, b0, pivmin, rr);
+                        int ca, cb;
+                        sturm_count2(d, e2, n, a0, b0, pivmin, ca, cb);
                         if (ca <= k && cb > k) { res = nt; done = true; break; }
                         if (ca > k) { hi = a0; chi = ca; } else { lo = a0; clo = ca; }
                         if (cb > k) { hi = fmin(hi, b0); chi = cb; } else { lo = fmax(lo, b0); clo = cb; }
@@ -846,27 +884,27 @@ __device__ __forceinline__ void stage_block(const C* __restrict__ a, const C* __
     const int t = threadIdx.x;
     const int i0 = j * ORM_NB;
     const int i1 = min(i0 + ORM_NB - 1, n - 2);
-    for (int idx = t; idx < (i1 + 1) * ORM_NB; idx += 256) {
+    for (int idx = t; idx < (i1 + 1) * ORM_NB; idx += blockDim.x) {
         const int r = idx / ORM_NB, k = idx % ORM_NB;
         const int i = i0 + k;
         C* dst = &vsb[r * ORM_VS + k];
         if (i <= n - 2 && r < i) cp_async_elem(dst, &a[(size_t)(i + 1) * n + r]);
         else *dst = (i <= n - 2 && r == i) ? cm<C>(1, 0) : cz<C>();
     }
-    cp_async_elem(&tsb[t], &tsrc[t]);
+    if (t < ORM_NB * ORM_NB) cp_async_elem(&tsb[t], &tsrc[t]);
     cp_async_commit();
 }
 
 // Apply all blocks to a chunk of CH columns of Z (row-major Z[r*n + col], real) and write
-// the chunk of X (column-major, column = eigenvector).  Thread t owns column t % CH and the
-// rows g + RG*q (g = t / CH, RG = 256/CH, q < ORM_RPT) in registers.  With dbuf the next
-// block's V and T are copied asynchronously while the current block is applied.
-template <int CH, class R>
-__global__ void __launch_bounds__(256)
+// the chunk of X (column-major, column = eigenvector).  NT threads; thread t owns column
+// t % CH and the rows g + RG*q (g = t / CH, RG = NT/CH, q < RPT) in registers.  With dbuf
+// the next block's V and T are copied asynchronously while the current block is applied.
+template <int CH, int NT, int RPT, class R>
+__global__ void __launch_bounds__(NT)
 k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __restrict__ Tw,
         const double* __restrict__ Z, typename Cx<R>::T* __restrict__ X, int n, int dbuf) {
     typedef typename Cx<R>::T C;
-    constexpr int RG = 256 / CH;
+    constexpr int RG = NT / CH, NW = NT / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* vsbuf[2];
     vsbuf[0] = reinterpret_cast<C*>(smem_raw);                    // [n][ORM_VS]
@@ -874,8 +912,8 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
     C* tsbuf[2];
     tsbuf[0] = vsbuf[0] + (size_t)(dbuf ? 2 : 1) * n * ORM_VS;       // [ORM_NB][ORM_NB]
     tsbuf[1] = dbuf ? tsbuf[0] + ORM_NB * ORM_NB : tsbuf[0];
-    C* wsum = tsbuf[0] + (size_t)(dbuf ? 2 : 1) * ORM_NB * ORM_NB;   // [8][ORM_NB][CH]
-    C* w2 = wsum + 8 * ORM_NB * CH;                                // [ORM_NB][CH]
+    C* wsum = tsbuf[0] + (size_t)(dbuf ? 2 : 1) * ORM_NB * ORM_NB;   // [NW][ORM_NB][CH]
+    C* w2 = wsum + NW * ORM_NB * CH;                               // [ORM_NB][CH]
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int c = t % CH, g = t / CH;
     const size_t mat = blockIdx.y;
@@ -884,9 +922,9 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
     const double* z = Z + mat * (size_t)n * n;
     const int nblk = (n - 1 + ORM_NB - 1) / ORM_NB;
     const C* tw = Tw + mat * (size_t)nblk * ORM_NB * ORM_NB;
-    C x[ORM_RPT];
+    C x[RPT];
 #pragma unroll
-    for (int q = 0; q < ORM_RPT; ++q) {
+    for (int q = 0; q < RPT; ++q) {
         const int r = g + RG * q;
         x[q] = (r < n && col < n) ? cm<C>(z[(size_t)r * n + col], 0) : cz<C>();
     }
@@ -914,7 +952,7 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
 #pragma unroll
         for (int k = 0; k < ORM_NB; ++k) wp[k] = cz<C>();
 #pragma unroll
-        for (int q = 0; q < ORM_RPT; ++q) {
+        for (int q = 0; q < RPT; ++q) {
             const int r = g + RG * q;
             if (r <= i1) {
                 const C* vr = vs + r * ORM_VS;
@@ -922,7 +960,7 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
                 for (int k = 0; k < ORM_NB; ++k) cfmac(wp[k], vr[k], x[q]);
             }
         }
-        // reduce over the row groups: inside the warp, then across the 8 warps
+        // reduce over the row groups: inside the warp, then across the NW warps
 #pragma unroll
         for (int s2 = CH; s2 < 32; s2 <<= 1)
 #pragma unroll
@@ -933,7 +971,7 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
         __syncthreads();
         C wk = cz<C>();
         if (t < ORM_NB * CH) {
-            for (int w8 = 0; w8 < 8; ++w8) wk = cadd(wk, wsum[w8 * ORM_NB * CH + t]);
+            for (int w8 = 0; w8 < NW; ++w8) wk = cadd(wk, wsum[w8 * ORM_NB * CH + t]);
             wsum[t] = wk;   // W[k][c] at t = k*CH + c (slot of warp 0, already read)
         }
         __syncthreads();
@@ -949,7 +987,7 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
 #pragma unroll
         for (int k = 0; k < ORM_NB; ++k) wc[k] = w2[k * CH + c];
 #pragma unroll
-        for (int q = 0; q < ORM_RPT; ++q) {
+        for (int q = 0; q < RPT; ++q) {
             const int r = g + RG * q;
             if (r <= i1) {
                 const C* vr = vs + r * ORM_VS;
@@ -964,14 +1002,14 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
     // write the chunk column-major through shared memory (coalesced along rows)
     C* xs = vsbuf[0];   // [CH][n]
 #pragma unroll
-    for (int q = 0; q < ORM_RPT; ++q) {
+    for (int q = 0; q < RPT; ++q) {
         const int r = g + RG * q;
         if (r < n) xs[(size_t)c * n + r] = x[q];
     }
     __syncthreads();
     C* xo = X + mat * (size_t)n * n;
     const int col0 = blockIdx.x * CH;
-    for (int idx = t; idx < CH * n; idx += 256) {
+    for (int idx = t; idx < CH * n; idx += NT) {
         const int cc = idx / n, r = idx % n;
         if (col0 + cc < n) xo[(size_t)(col0 + cc) * n + r] = xs[idx];
     }
@@ -1795,10 +1833,11 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     p.ch = ch;
-    size_t smem = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * ce;
+    const int onw = 8;   // warps of k_ormtr (256 threads; 512 threads of 8 rows measured slower)
+    size_t smem = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + onw * ORM_NB * ch + ORM_NB * ch) * ce;
     p.dbuf = smem <= 220 * 1024 ? 1 : 0;
     if (!p.dbuf)
-        smem = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + 8 * ORM_NB * ch + ORM_NB * ch) * ce;
+        smem = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + onw * ORM_NB * ch + ORM_NB * ch) * ce;
     p.smem_orm = smem;
     // register-resident k_ormtr up to order 383 (it fits and beats the GEMM path there), the
     // GEMM path from 384 on
@@ -1893,8 +1932,9 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
     const int n = p.n;
     const size_t nn = (size_t)n * n;
     if (p.small_bt) {
-        auto ormtr = p.ch == 16 ? k_ormtr<16, R> : p.ch == 8 ? k_ormtr<8, R> : p.ch == 4 ? k_ormtr<4, R>
-                   : p.ch == 2 ? k_ormtr<2, R> : k_ormtr<1, R>;
+        auto ormtr = p.ch == 16 ? k_ormtr<16, 256, ORM_RPT, R> : p.ch == 8 ? k_ormtr<8, 256, ORM_RPT, R>
+                   : p.ch == 4 ? k_ormtr<4, 256, ORM_RPT, R> : p.ch == 2 ? k_ormtr<2, 256, ORM_RPT, R>
+                   : k_ormtr<1, 256, ORM_RPT, R>;
         if (cudaFuncSetAttribute(ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_orm) != cudaSuccess)
             return RLMB_ERR_CUDA;
         if (n > 1) {
