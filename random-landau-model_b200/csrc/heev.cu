@@ -1225,7 +1225,8 @@ static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked re
 
 // p += A v for the Hermitian leading m x m block stored in the upper triangle of a
 // (column-major, leading dimension ld; read only), v and p in shared memory.  Work is dealt
-// to warps as strips of HV_W columns; a lane holds one row of a 32-row block of the strip:
+// to warps as strips of HV_W columns (dealt back and forth for balance); a lane holds one
+// row of a 32-row block of the strip:
 // its row contributions go to p[r] (shared atomics, once per block), its column
 // contributions conj(A[r][c]) v[r] stay in registers for the whole strip and are reduced
 // across the warp once at the end.  Interior blocks (entirely above the diagonal and inside
@@ -1237,7 +1238,11 @@ __device__ __forceinline__ void hemv_upper(const C* __restrict__ a, int ld, int 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = NT / 32;
     const int nstrips = (m + HV_W - 1) / HV_W;
-    for (int s = warp; s < nstrips; s += NW) {
+    // strip s holds s*HV_W/32 + 1 row blocks: deal them back and forth (warp w takes strips
+    // w, 2NW-1-w, 2NW+w, ...) so that every warp gets a similar amount of work
+    for (int base = 0; base < nstrips; base += NW) {
+        const int s = ((base / NW) & 1) ? base + NW - 1 - warp : base + warp;
+        if (s >= nstrips) continue;
         const int c0 = s * HV_W;
         C vc[HV_W], e[HV_W];
 #pragma unroll
@@ -1777,7 +1782,7 @@ static HetrdCfg hetrd_config(int n) {
     const size_t ce = 2 * sizeof(R);   // complex element
     const size_t tri_full = (size_t)n * (n + 1) / 2;
     const size_t vec128 = 4 * (size_t)n * ce + 2 * (128 / 32) * sizeof(R);
-    if (vec128 + tri_full * ce <= 76 * 1024) return {128, (int)tri_full, vec128 + tri_full * ce};
+    if (vec128 + tri_full * ce <= 110 * 1024) return {128, (int)tri_full, vec128 + tri_full * ce};
     const size_t vec512 = 4 * (size_t)n * ce + 2 * (512 / 32) * sizeof(R);
     const size_t budget = 220 * 1024;
     size_t cap = budget > vec512 ? (budget - vec512) / ce : 0;
