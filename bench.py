@@ -439,6 +439,55 @@ def run_gpu_rlm(args):
     print(json.dumps(line), flush=True)
 
 
+FSS_SIZES = (64, 128, 192, 256, 384, 512)
+
+
+def run_gpu_fss(args):
+    """Finite-size-scaling workload: rlm with n_phi in FSS_SIZES, 16 samples each, g=16,
+    impurity concentration 16 -- one rlmb_rlm_mesh_solve call per size per step (FP64).
+    Reports k-point solves/s per size and for the whole step, and each size's eigensolver
+    throughput against the FP64 roofline (13.33 n^3 flops per solve)."""
+    import torch
+    import rlmb
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    g, ns = 16, 16
+    kpts = (g + 1) ** 2
+    ctx = rlmb.Context(local)
+    peak = ctx.fp64_peak_tflops()
+    per = {}
+    for n in FSS_SIZES:
+        for _ in range(args.warmup):
+            ctx.rlm_mesh_solve(n, 1.0, 16.0, g, SEED, 0, ns)
+        ctx.profile(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for st in range(args.steps):
+            ctx.rlm_mesh_solve(n, 1.0, 16.0, g, SEED, ns * (st + 1), ns)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        prof = ctx.profile_report()
+        ctx.profile(False)
+        eig_ms = sum(prof.get(k, (0, 0))[0] for k in ("k_hetrd", "k_stebz", "k_stein", "k_larft", "k_ormtr"))
+        solves = ns * kpts * args.steps
+        eig_tf = 13.33 * n ** 3 * solves / (eig_ms * 1e-3) / 1e12
+        per[str(n)] = {"solves_per_s": solves / dt, "ms_per_step": 1e3 * dt / args.steps,
+                       "eigensolve_tflops": eig_tf, "eigensolve_frac_of_fp64_peak": eig_tf / peak}
+    total_solves = len(FSS_SIZES) * ns * kpts * args.steps
+    total_s = sum(v["ms_per_step"] for v in per.values()) * args.steps / 1e3
+    line = {"metric": METRIC, "value": total_solves / total_s, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "rlm finite-size scaling: n_phi in " + ",".join(map(str, FSS_SIZES)) +
+                                   f", {ns} samples each per step, g={g}, impurity concentration 16, seed {SEED}",
+                       "api": "rlmb_rlm_mesh_solve per size (sizes run one after another)"},
+            "per_size": per, "fp64_peak_tflops": peak}
+    ctx.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_probe(args):
     """One rlmb_heevd_batched call on `batch` random Hermitian matrices of order n (the small
     case the ncu captures under profiles/ are taken on)."""
@@ -461,8 +510,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="hlm48x16", choices=["hlm48x16"] + sorted(RLM_WORKLOADS),
-                    help="hlm48x16 (default, the headline), or an rlm configuration (1 GPU, both precisions)")
+    ap.add_argument("--workload", default="hlm48x16", choices=["hlm48x16", "fss"] + sorted(RLM_WORKLOADS),
+                    help="hlm48x16 (default, the headline), an rlm configuration (1 GPU, both precisions), "
+                         "or fss (the rlm finite-size-scaling sizes, 1 GPU)")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision measurement on the same inputs")
     ap.add_argument("--probe", default=None, choices=["heevd"],
@@ -476,6 +526,8 @@ def main():
         run_reference(args)
     elif args.workload in RLM_WORKLOADS:
         run_gpu_rlm(args)
+    elif args.workload == "fss":
+        run_gpu_fss(args)
     else:
         run_gpu(args)
 
