@@ -666,8 +666,9 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
         }
     }
     __syncthreads();
-    // ---- eigenvectors: isolated eigenvalues by one twisted solve; clusters by inverse
-    //      iteration with modified Gram-Schmidt, handled by the leader's thread
+    // ---- eigenvectors: isolated eigenvalues by one twisted solve; clusters (handled by the
+    //      leader's thread) by twisted solves + modified Gram-Schmidt when their members are
+    //      still separated, else by inverse iteration with modified Gram-Schmidt
     const double eps = DBL_EPSILON;
     const double dtpcrt = sqrt(0.1 / n);
     for (int k0 = tid; k0 < n; k0 += TRI_THREADS) {
@@ -676,6 +677,31 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
         while (k1 + 1 < n && leader[k1 + 1] == k0) ++k1;
         if (k1 == k0) {
             twisted_vector(d, e, e2, n, lam[k0], pivmin, z, k0, la, lb, tid);
+            continue;
+        }
+        // a cluster whose members are still 1e-9 * ||T|| apart: each twisted vector is
+        // accurate to ~eps ||T|| / gap, so a twisted solve per member followed by modified
+        // Gram-Schmidt inside the cluster replaces the iterations
+        double mingap = DBL_MAX;
+        for (int k = k0 + 1; k <= k1; ++k) mingap = fmin(mingap, lam[k] - lam[k - 1]);
+        if (mingap > 1e-9 * onenrm) {
+            for (int k = k0; k <= k1; ++k) {
+                twisted_vector(d, e, e2, n, lam[k], pivmin, z, k, la, lb, tid);
+                for (int q = k0; q < k; ++q) {
+                    double dot = 0.0;
+                    for (int j = 0; j < n; ++j) dot += z[(size_t)j * n + q] * z[(size_t)j * n + k];
+                    for (int j = 0; j < n; ++j) z[(size_t)j * n + k] -= dot * z[(size_t)j * n + q];
+                }
+                double x2s = 0.0, big = 0.0;
+                for (int j = 0; j < n; ++j) {
+                    const double t = z[(size_t)j * n + k];
+                    x2s += t * t;
+                    if (fabs(t) > fabs(big)) big = t;
+                }
+                double rn = 1.0 / sqrt(fmax(x2s, DBL_MIN));
+                if (big < 0.0) rn = -rn;
+                for (int j = 0; j < n; ++j) z[(size_t)j * n + k] *= rn;
+            }
             continue;
         }
         double xjm = lam[k0];
