@@ -337,7 +337,11 @@ def run_gpu(args):
                     "traffic": tr * matrices_per_launch if tr is not None else None,
                     "peak_source": "measured in this run: FP64 FMA throughput probe "
                                    "(MEASURED_PEAKS.json holds no FP64 figure)",
-                    "share_of_gpu_time": kms / total_ms}
+                    "share_of_gpu_time": kms / total_ms,
+                    "launches": klaunch,
+                    "note": "per launch = averaged over the label's launches (k_hetrd covers the panel "
+                            "kernels, their GEMM updates and the unblocked tail); traffic = ncu DRAM bytes "
+                            "per matrix (profiles/dram_traffic.json) x matrices per launch"}
         eig_ms = sum(prof.get(k, (0, 0))[0] for k in ("k_hetrd", "k_stebz", "k_stein", "k_larft", "k_ormtr"))
         eig_tflops = 13.33 * N_PHI ** 3 * SOLVES_PER_STEP * args.steps / (eig_ms * 1e-3) / 1e12
         line = {
