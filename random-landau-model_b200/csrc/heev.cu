@@ -925,8 +925,8 @@ __device__ __forceinline__ void stage_block(const C* __restrict__ a, const C* __
 // the chunk of X (column-major, column = eigenvector).  NT threads; thread t owns column
 // t % CH and the rows g + RG*q (g = t / CH, RG = NT/CH, q < RPT) in registers.  With dbuf
 // the next block's V and T are copied asynchronously while the current block is applied.
-template <int CH, int NT, int RPT, class R>
-__global__ void __launch_bounds__(NT)
+template <int CH, int NT, int RPT, class R, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB)
 k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __restrict__ Tw,
         const double* __restrict__ Z, typename Cx<R>::T* __restrict__ X, int n, int dbuf) {
     typedef typename Cx<R>::T C;
@@ -1246,7 +1246,7 @@ struct EpSub {     // X(r, c) -= acc
 // over all SMs (k_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
 // k_hetrd.  D, E, TAU and the reflector storage are those of the unblocked reduction.
 static constexpr int HP_W = 32;      // panel width
-static constexpr int HT_TAIL = 96;   // order below which the unblocked kernel finishes
+static constexpr int HT_TAIL = 64;   // order below which the unblocked kernel finishes
 static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
 
 // p += A v for the Hermitian leading m x m block stored in the upper triangle of a
@@ -1864,7 +1864,8 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     p.ch = ch;
-    const int onw = 8;   // warps of k_ormtr (256 threads; 512 threads of 8 rows measured slower)
+    const int onw = 8;   // warps of k_ormtr (256 threads; 512 threads of 8 rows, or 8 columns
+                         // of 8 rows at two CTAs per SM, measured slower)
     size_t smem = ((size_t)2 * n * ORM_VS + 2 * ORM_NB * ORM_NB + onw * ORM_NB * ch + ORM_NB * ch) * ce;
     p.dbuf = smem <= 220 * 1024 ? 1 : 0;
     if (!p.dbuf)
