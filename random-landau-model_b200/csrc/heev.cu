@@ -1,20 +1,25 @@
-// Batched complex Hermitian eigensolver, double precision (sm_100a).
+// Batched complex Hermitian eigensolver (sm_100a), double precision or mixed precision.
 //
 // Replaces the reference's dense solver calls: mkl_heevd (diag_wrappers/mkl_diag.cpp:2-9,
 // LAPACKE_zheevd col-major 'U'), cusolver_diag_hamil (diag_wrappers/cusolver_diag.cu:3-22)
 // and magma_diag_hamil (diag_wrappers/magma_diag.cu:2-49).  The LAPACK arithmetic those
-// calls reach is restated from its published algorithms, in three kernels per batch:
+// calls reach is restated from its published algorithms:
 //
-//   k_hetrd   Householder reduction A = Q T Q^H (LAPACK zhetd2, uplo='U'): one CTA per
-//             matrix, the matrix itself in global memory (L2 resident while its CTA
-//             runs); per column a reflector (zlarfg), a Hermitian matrix-vector product
-//             over 32x32 tiles that reads every stored element once and uses it for
-//             both the row and the transposed contribution, and a rank-2 update.
-//   k_tridiag Eigenvalues of T by Sturm-count bisection (one thread per eigenvalue,
-//             LAPACK dstebz), eigenvectors by inverse iteration with partial-pivoting
-//             LU of T - lambda I and modified Gram-Schmidt inside clusters (dstein).
-//   k_ormtr   Back-transformation X = Q Z (zunmtr): one CTA per (matrix, 16-column
-//             chunk of Z) holding the chunk in shared memory.
+//   reduction      A = Q T Q^H (zhetrd, uplo='U').  From order 256: panels of 32 columns
+//                  (k_hetrd_panel, zlatrd restated, one CTA per matrix) whose rank-64
+//                  updates run as batched GEMMs over all SMs (k_zgemm); the last leading
+//                  block (order <= 64, or all of a smaller matrix) by the unblocked,
+//                  look-ahead k_hetrd (zhetd2), its triangle resident in shared memory.
+//   tridiagonal    k_tridiag: eigenvalues by Sturm counts (dstebz restated, seeded from a
+//                  shared grid, Newton-accelerated); eigenvectors by twisted factorisation,
+//                  or for clusters inverse iteration / twisted solves with modified
+//                  Gram-Schmidt (dstein restated).
+//   back-transform X = Q Z (zunmtr): k_larft + k_ormtr (register-resident Z chunks, blocks
+//                  of 16 reflectors) below order 384, else T factors from batched Gram
+//                  GEMMs and three k_zgemm launches per block of 64 reflectors.
+//   mixed mode     the reduction and back-transformation in single precision, then double
+//                  refinement of every eigenpair (k_ref_*, Ogita-Aishima restated, with
+//                  cluster Rayleigh-Ritz).
 //
 // Every wait is a __syncthreads inside one CTA: no inter-CTA dependencies, no spins.
 #include "common.cuh"
