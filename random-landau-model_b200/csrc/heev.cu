@@ -1262,7 +1262,7 @@ static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked re
 // contributions conj(A[r][c]) v[r] stay in registers for the whole strip and are reduced
 // across the warp once at the end.  Interior blocks (entirely above the diagonal and inside
 // the matrix) run without predicates.
-static constexpr int HV_W = 4;
+static constexpr int HV_W = 8;
 template <int NT, class C>
 __device__ __forceinline__ void hemv_upper(const C* __restrict__ a, int ld, int m, const C* __restrict__ v,
                                            C* p) {
@@ -1332,7 +1332,7 @@ __device__ __forceinline__ void hemv_upper(const C* __restrict__ a, int ld, int 
 }
 
 template <int NT, class R>
-__global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 4)
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
 k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
               typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ PV,
               typename Cx<R>::T* __restrict__ PW, int n, int m) {
