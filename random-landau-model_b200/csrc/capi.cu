@@ -118,8 +118,16 @@ static size_t mesh_budget_bytes(int device) {
         return (size_t)8 << 30;
     }
     (void)device;
-    const size_t cap = (size_t)24 << 30;
+    const size_t cap = (size_t)40 << 30;
     return std::min(cap, free_b / 3);
+}
+
+// Samples per batch: at most `fit`, and the batches of one call equal in size (a short last
+// batch would leave most SMs idle in the one-CTA-per-matrix kernels).
+static int balanced_batch(int n_samples, size_t fit) {
+    const size_t cap = std::max<size_t>(1, std::min<size_t>((size_t)n_samples, fit));
+    const size_t nbatches = ((size_t)n_samples + cap - 1) / cap;
+    return (int)(((size_t)n_samples + nbatches - 1) / nbatches);
 }
 
 }  // namespace rlmb
@@ -400,7 +408,7 @@ static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_me
     // batch of samples that fits the budget
     const size_t per_sample = kpts * (nn * sizeof(cplx) + (size_t)n_phi * (sizeof(double) + 2 * sizeof(cplx))) +
                               (size_t)dim * dim * sizeof(cplx) + 3 * (size_t)nimp * sizeof(double);
-    int nb = (int)std::max<size_t>(1, std::min<size_t>(n_samples, mesh_budget_bytes(ctx->device) / per_sample));
+    int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx->device) / per_sample);
     size_t bytes = 0;
     need<cplx>(bytes, cmn.size() / 2);
     need<cplx>(bytes, cmt.size() / 2);
@@ -490,7 +498,7 @@ int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int ban
     if (int rc = hlm_tables(ctx, lx, ly, Q, band, g, &hb)) return rc;
     const size_t per_sample = kpts * (nn * sizeof(cplx) + (size_t)N * (sizeof(double) + 2 * sizeof(cplx))) +
                               (size_t)ns * sizeof(cplx);
-    const int nb = (int)std::max<size_t>(1, std::min<size_t>(n_samples, mesh_budget_bytes(ctx->device) / per_sample));
+    const int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx->device) / per_sample);
     size_t bytes = 0;
     need<int>(bytes, kpts);
     need<cplx>(bytes, (size_t)ns * nb);

@@ -1931,11 +1931,20 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
     int m = n;
     if (p.npanels > 0) {
         C* PWb = PV + (size_t)nb * HP_W * n;
-        // 256 threads (two CTAs per SM) for orders 385..512, 512 threads otherwise (measured)
-        const bool mid = n > 384 && n <= 512;
+        // 256 threads (two CTAs per SM) for orders 385..512, 512 threads otherwise (measured);
+        // above order 512 also 256 threads when the chunk has more matrices than SMs but
+        // fits two per SM: all of it is then resident at once instead of in two waves
+        auto smem_of = [&](int nt) { return (2 * (size_t)n + 2 * HP_W) * sizeof(C) + 2 * (nt / 32) * sizeof(R); };
+        bool mid = n > 384 && n <= 512;
+        if (n > 512) {
+            int dev = 0, sms = 148;
+            if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+                return RLMB_ERR_CUDA;
+            mid = nb > sms && nb <= 2 * sms && smem_of(256) <= 113 * 1024;
+        }
         auto panel = mid ? k_hetrd_panel<256, R> : k_hetrd_panel<512, R>;
         const int pnt = mid ? 256 : 512;
-        const size_t smem = (2 * (size_t)n + 2 * HP_W) * sizeof(C) + 2 * (pnt / 32) * sizeof(R);
+        const size_t smem = smem_of(pnt);
         if (cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return RLMB_ERR_CUDA;
         for (int k = 0; k < p.npanels; ++k) {
@@ -2171,6 +2180,9 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     size_t chunk = std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)batch));
     chunk = std::min<size_t>(chunk, 65535);   // grid y / z extent of the per-matrix launches
     if (!plan.small_bt) chunk = std::min<size_t>(chunk, 65535 / std::max(plan.nblk64, 1));   // (matrix, block) batches
+    // equal chunks: a short last chunk would leave most SMs idle in the one-CTA-per-matrix kernels
+    const size_t nchunks = (batch + chunk - 1) / chunk;
+    chunk = (batch + nchunks - 1) / nchunks;
     if (int rc = ensure_workspace(ctx, chunk * per)) return rc;
     const size_t nn = (size_t)n * n;
     long long unused = 0;

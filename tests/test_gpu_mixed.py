@@ -58,7 +58,7 @@ def _check(M, w, X, wref):
     return err, res, orth
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 33, 64, 128, 256, 512, 800, 1000])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 33, 64, 128, 200, 256, 300, 512, 800, 1000])
 def test_mixed_heevd_random(ctx, n):
     rng = np.random.default_rng(1000 + n)
     mats = [_hermitian(rng, n) for _ in range(3 if n <= 512 else 2)]
@@ -68,7 +68,7 @@ def test_mixed_heevd_random(ctx, n):
 
 
 @pytest.mark.parametrize("kind", ["identity", "degenerate", "diagonal", "zero", "blocks", "tridiag_split"])
-@pytest.mark.parametrize("n", [7, 48])
+@pytest.mark.parametrize("n", [7, 48, 160, 300])
 def test_mixed_heevd_structured(ctx, kind, n):
     rng = np.random.default_rng(11 * n)
     M = _hermitian(rng, n, kind)

@@ -82,7 +82,7 @@ def _run_heevd(ctx, mats):
     return w.cpu().numpy(), [X[b].T for b in range(len(mats))]
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 31, 32, 33, 64, 100, 128, 256])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 31, 32, 33, 64, 100, 128, 129, 200, 256, 300, 384, 457, 512])
 def test_heevd_random(ctx, n):
     rng = np.random.default_rng(n)
     mats = [_hermitian(rng, n) for _ in range(3)]
@@ -109,7 +109,7 @@ def test_heevd_large_orders(ctx, n):
 
 
 @pytest.mark.parametrize("kind", ["identity", "degenerate", "diagonal", "zero", "blocks", "tridiag_split"])
-@pytest.mark.parametrize("n", [7, 48])
+@pytest.mark.parametrize("n", [7, 48, 160, 300])
 def test_heevd_structured(ctx, kind, n):
     rng = np.random.default_rng(7 * n)
     M = _hermitian(rng, n, kind)
