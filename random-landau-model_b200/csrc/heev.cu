@@ -7,7 +7,7 @@
 //
 //   reduction      A = Q T Q^H (zhetrd, uplo='U').  From order 256: panels of 32 columns
 //                  (k_hetrd_panel, zlatrd restated, one CTA per matrix) whose rank-64
-//                  updates run as batched GEMMs over all SMs (k_zgemm); the last leading
+//                  updates run as batched GEMMs over all SMs (launch_zgemm); the last leading
 //                  block (order <= 64, or all of a smaller matrix) by the unblocked,
 //                  look-ahead k_hetrd (zhetd2), its triangle resident in shared memory.
 //   tridiagonal    k_tridiag: eigenvalues by Sturm counts (dstebz restated, seeded from a
@@ -15,8 +15,8 @@
 //                  or for clusters inverse iteration / twisted solves with modified
 //                  Gram-Schmidt (dstein restated).
 //   back-transform X = Q Z (zunmtr): k_larft + k_ormtr (register-resident Z chunks, blocks
-//                  of 16 reflectors) below order 384, else T factors from batched Gram
-//                  GEMMs and three k_zgemm launches per block of 64 reflectors.
+//                  of 16 reflectors) below order 256, else T factors from batched Gram
+//                  GEMMs and three GEMM launches per block of 64 reflectors.
 //   mixed mode     the reduction and back-transformation in single precision, then double
 //                  refinement of every eigenpair (k_ref_*, Ogita-Aishima restated, with
 //                  cluster Rayleigh-Ritz).
@@ -1053,43 +1053,44 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
 // global memory (column-major, column = eigenvector) and is read twice and written once
 // per block.
 static constexpr int BT_NB = 64;
-static constexpr int BT_GEMM_MIN = 384;   // order from which the GEMM back-transformation runs
+static constexpr int BT_GEMM_MIN = 256;   // order from which the GEMM back-transformation runs
 
 // T factor of block j (reflectors 64j .. 64j+63) of one matrix from its Gram matrix
 // G = V_j^H V_j (column-major 64 x 64, computed by a batched GEMM into the same slot of Tw):
 //   T[k][k] = tau_k,  T[k][q] = -tau_k sum_{l=q}^{k-1} G[k][l] T[l][q]   (q < k),
-// written back row-major (T[k][q] at k*64 + q); grid (blocks, matrices), 64 threads.
+// written back row-major (T[k][q] at k*64 + q); grid (blocks, matrices), 128 threads.
+// The recurrence reads G only above its diagonal (S[l][k], l < k, with S[l][k] = G[k][l])
+// and T only on and below it, so T overwrites the lower half of the one shared table S as
+// it is formed.  Two threads share row q of T (even and odd l), halving the dependent chain.
 template <class R>
-__global__ void __launch_bounds__(64)
+__global__ void __launch_bounds__(2 * BT_NB)
 k_larft64(const typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ Tw, int n) {
     typedef typename Cx<R>::T C;
     typedef C Row[BT_NB + 1];
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Row* G = reinterpret_cast<Row*>(smem_raw);   // G[l][k] = v_k^H v_l (column l of the Gram matrix)
-    Row* T = G + BT_NB;
-    const int j = blockIdx.x, q = threadIdx.x;
+    Row* S = reinterpret_cast<Row*>(smem_raw);   // S[l][k] = G[k][l] (l < k); T[k][q] at S[k][q] (q <= k)
+    const int j = blockIdx.x, q = threadIdx.x >> 1, h = threadIdx.x & 1;
     const size_t mat = blockIdx.y;
     const C* tau = TAU + mat * n;
     const int nblk = (n - 1 + BT_NB - 1) / BT_NB;
     const int i0 = j * BT_NB;
     C* blk = Tw + (mat * nblk + j) * BT_NB * BT_NB;
-    for (int l = 0; l < BT_NB; ++l) G[l][q] = blk[l * BT_NB + q];
+    for (int idx = threadIdx.x; idx < BT_NB * BT_NB; idx += 2 * BT_NB) S[idx / BT_NB][idx % BT_NB] = blk[idx];
     __syncthreads();
     for (int k = 0; k < BT_NB; ++k) {
         const int ik = i0 + k;
         const C tk = ik <= n - 2 ? tau[ik] : cz<C>();
-        C val = cz<C>();
-        if (q == k) {
-            val = tk;
-        } else if (q < k) {
-            C sum = cz<C>();
-            for (int l = q; l < k; ++l) cfma(sum, G[l][k], T[l][q]);
-            val = cscale(cmul(tk, sum), (R)-1);
-        }
-        T[k][q] = val;
+        C sum = cz<C>();
+        if (q < k)
+            for (int l = q + h; l < k; l += 2) cfma(sum, S[l][k], S[l][q]);
+        sum = cadd(sum, shfl_xor(sum, 1));
+        if (h == 0 && q <= k) S[k][q] = q == k ? tk : cscale(cmul(tk, sum), (R)-1);
         __syncthreads();
     }
-    for (int k = 0; k < BT_NB; ++k) blk[k * BT_NB + q] = T[k][q];
+    for (int idx = threadIdx.x; idx < BT_NB * BT_NB; idx += 2 * BT_NB) {
+        const int k = idx / BT_NB, c = idx % BT_NB;
+        blk[idx] = c <= k ? S[k][c] : cz<C>();
+    }
 }
 
 // Z (row-major real) -> X (column-major complex), grid-stride over all batch entries.
@@ -1875,8 +1876,8 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
     if (!p.dbuf)
         smem = ((size_t)std::max(n * ORM_VS, n * ch) + ORM_NB * ORM_NB + onw * ORM_NB * ch + ORM_NB * ch) * ce;
     p.smem_orm = smem;
-    // register-resident k_ormtr up to order 383 (it fits and beats the GEMM path there), the
-    // GEMM path from 384 on
+    // register-resident k_ormtr up to order 255 (it beats the GEMM path there), the GEMM path
+    // (double precision on the DMMA engine) from 256 on
     p.small_bt = n < BT_GEMM_MIN && (n + 256 / ch - 1) / (256 / ch) <= ORM_RPT && smem <= 220 * 1024;
     const size_t nn = (size_t)n * n;
     auto r256 = [](size_t v) { return (v + 255) / 256 * 256; };
@@ -1997,11 +1998,11 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
                             EpStore<C>{Tw, BT_NB, (size_t)BT_NB * BT_NB}, BT_NB, BT_NB, n, nb * p.nblk64) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
-    const size_t smem_t = 2 * BT_NB * (BT_NB + 1) * sizeof(C);
+    const size_t smem_t = BT_NB * (BT_NB + 1) * sizeof(C);
     if (cudaFuncSetAttribute(k_larft64<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_PROF("k_larft");
-    k_larft64<R><<<dim3(p.nblk64, nb), BT_NB, smem_t, st>>>(TAUw, Tw, n);
+    k_larft64<R><<<dim3(p.nblk64, nb), 2 * BT_NB, smem_t, st>>>(TAUw, Tw, n);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ormtr");
     k_z_to_x<C><<<2048, 256, 0, st>>>(Zw, Xw, n, (size_t)nb * nn);
