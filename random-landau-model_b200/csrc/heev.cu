@@ -2027,7 +2027,9 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
             return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
         RLMB_CHUNK_PROF("k_ormtr");
-        if (launch_zgemm<C, 128>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs}, EpSub<C>{Xw, n},
+        // X -= V W': 64-row tiles (two CTAs per SM) on the DMMA engine, 128 in single precision
+        constexpr int BMX = std::is_same<C, cplx>::value ? 64 : 128;
+        if (launch_zgemm<C, BMX>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs}, EpSub<C>{Xw, n},
                                  rows, n, BT_NB, nb) != cudaSuccess)
             return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
