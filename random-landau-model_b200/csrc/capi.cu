@@ -110,16 +110,17 @@ static bool hlm_args_ok(int lx, int ly, int Q, int band, int g) {
            g > 0 && lx / Q <= 64 && ly <= 64;
 }
 
-// Device memory budget for one batch of mesh data.
-static size_t mesh_budget_bytes(int device) {
+// Device memory budget for one batch of mesh data: a third of the free memory, counting the
+// context's own pipeline buffer (reused by the batch) as free so that repeated calls batch
+// alike, at most 40 GB.
+static size_t mesh_budget_bytes(const rlmb_context* ctx) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         cudaGetLastError();
         return (size_t)8 << 30;
     }
-    (void)device;
     const size_t cap = (size_t)40 << 30;
-    return std::min(cap, free_b / 3);
+    return std::min(cap, (free_b + ctx->pipe_bytes) / 3);
 }
 
 // Samples per batch: at most `fit`, and the batches of one call equal in size (a short last
@@ -408,7 +409,7 @@ static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_me
     // batch of samples that fits the budget
     const size_t per_sample = kpts * (nn * sizeof(cplx) + (size_t)n_phi * (sizeof(double) + 2 * sizeof(cplx))) +
                               (size_t)dim * dim * sizeof(cplx) + 3 * (size_t)nimp * sizeof(double);
-    int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx->device) / per_sample);
+    int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx) / per_sample);
     size_t bytes = 0;
     need<cplx>(bytes, cmn.size() / 2);
     need<cplx>(bytes, cmt.size() / 2);
@@ -498,7 +499,7 @@ int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int ban
     if (int rc = hlm_tables(ctx, lx, ly, Q, band, g, &hb)) return rc;
     const size_t per_sample = kpts * (nn * sizeof(cplx) + (size_t)N * (sizeof(double) + 2 * sizeof(cplx))) +
                               (size_t)ns * sizeof(cplx);
-    const int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx->device) / per_sample);
+    const int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx) / per_sample);
     size_t bytes = 0;
     need<int>(bytes, kpts);
     need<cplx>(bytes, (size_t)ns * nb);

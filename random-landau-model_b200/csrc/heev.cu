@@ -1620,39 +1620,11 @@ struct EpCoupling {
 // first index): G = X_C^H X_C and E = X_C^H R_C by warp sums in double, S = E + G Lambda
 // (Hermitian part), then in one lane G = L L^H, C = L^-1 S L^-H, Jacobi C = V diag(mu) V^H,
 // Y = L^-H V (ascending mu).  Y[j][p] (column j's coefficients) and mu[j] go to YB / MU.
-template <class XT>
-__global__ void k_ref_cluster_solve(const XT* __restrict__ X, const cplx* __restrict__ Res,
-                                    const double* __restrict__ W, const int2* __restrict__ CL,
-                                    cplx* __restrict__ YB, double* __restrict__ MU, int n, int nmat) {
-    const int lane = threadIdx.x & 31;
-    const size_t gw = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    if (gw >= (size_t)nmat * n) return;
-    const size_t mat = gw / n;
-    const int a = (int)(gw % n);
-    const int2 c = CL[mat * n + a];
-    const int k = c.y;
-    if (c.x != a || k < 2 || k > RF_KMAX) return;
-    const XT* x = X + mat * (size_t)n * n;
-    const cplx* res = Res + mat * (size_t)n * n;
-    const double* w = W + mat * n;
-    cplx G[RF_KMAX * RF_KMAX], S[RF_KMAX * RF_KMAX];   // column-major [p + q*k]
-    for (int p = 0; p < k; ++p)
-        for (int q = 0; q < k; ++q) {
-            const XT* xp = x + (size_t)(a + p) * n;
-            const XT* xq = x + (size_t)(a + q) * n;
-            const cplx* rq = res + (size_t)(a + q) * n;
-            cplx g = mk(0, 0), e = mk(0, 0);
-            for (int r = lane; r < n; r += 32) {
-                const cplx xpr = to_c64(xp[r]);
-                cfmac(g, xpr, to_c64(xq[r]));
-                cfmac(e, xpr, rq[r]);
-            }
-            g = warp_sum(g);
-            e = warp_sum(e);
-            G[p + q * k] = g;
-            S[p + q * k] = mk(e.x + w[a + q] * g.x, e.y + w[a + q] * g.y);
-        }
-    if (lane != 0) return;
+// Lane 0's part of k_ref_cluster_solve for the cluster of k members starting at eigenpair a
+// of matrix mat: G (Gram) and S (Rayleigh) of the cluster in, Y and mu out.
+__device__ __noinline__ void cluster_rr_serial(cplx* G, cplx* S, cplx* T, int k, size_t mat, int a, int n,
+                                               const double* __restrict__ w, cplx* __restrict__ YB,
+                                               double* __restrict__ MU) {
     // Hermitian parts
     for (int p = 0; p < k; ++p)
         for (int q = p; q < k; ++q) {
@@ -1684,7 +1656,6 @@ __global__ void k_ref_cluster_solve(const XT* __restrict__ X, const cplx* __rest
         }
     }
     // T = L^-1 S (columns), then C = L^-1 T^H  (= L^-1 S L^-H, Hermitian)
-    cplx T[RF_KMAX * RF_KMAX];
     for (int q = 0; q < k; ++q)
         for (int i = 0; i < k; ++i) {
             cplx s = S[i + q * k];
@@ -1727,6 +1698,52 @@ __global__ void k_ref_cluster_solve(const XT* __restrict__ X, const cplx* __rest
         cplx* yo = YB + (mat * n + a + q) * RF_KMAX;
         for (int p = 0; p < k; ++p) yo[p] = y[p];
         MU[mat * n + a + q] = S[col * (k + 1)].x;
+    }
+}
+
+template <class XT>
+__global__ void k_ref_cluster_solve(const XT* __restrict__ X, const cplx* __restrict__ Res,
+                                    const double* __restrict__ W, const int2* __restrict__ CL,
+                                    cplx* __restrict__ YB, double* __restrict__ MU, int n, int nmat) {
+    const int lane = threadIdx.x & 31;
+    // G, S and T of this warp's cluster in shared memory (column-major [p + q*k]); only lane 0
+    // writes and reads them
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx* G = reinterpret_cast<cplx*>(smem_raw) + (size_t)(threadIdx.x / 32) * 3 * RF_KMAX * RF_KMAX;
+    cplx* S = G + RF_KMAX * RF_KMAX;
+    cplx* T = S + RF_KMAX * RF_KMAX;
+    // grid-stride over the eigenpairs: most are not cluster leaders and are skipped at once
+    const size_t nwarps = (size_t)gridDim.x * (blockDim.x / 32);
+    for (size_t gw = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; gw < (size_t)nmat * n;
+         gw += nwarps) {
+        const size_t mat = gw / n;
+        const int a = (int)(gw % n);
+        const int2 c = CL[mat * n + a];
+        const int k = c.y;
+        if (c.x != a || k < 2 || k > RF_KMAX) continue;
+        const XT* x = X + mat * (size_t)n * n;
+        const cplx* res = Res + mat * (size_t)n * n;
+        const double* w = W + mat * n;
+        for (int p = 0; p < k; ++p)
+            for (int q = 0; q < k; ++q) {
+                const XT* xp = x + (size_t)(a + p) * n;
+                const XT* xq = x + (size_t)(a + q) * n;
+                const cplx* rq = res + (size_t)(a + q) * n;
+                cplx g = mk(0, 0), e = mk(0, 0);
+                for (int r = lane; r < n; r += 32) {
+                    const cplx xpr = to_c64(xp[r]);
+                    cfmac(g, xpr, to_c64(xq[r]));
+                    cfmac(e, xpr, rq[r]);
+                }
+                g = warp_sum(g);
+                e = warp_sum(e);
+                if (lane == 0) {
+                    G[p + q * k] = g;
+                    S[p + q * k] = mk(e.x + w[a + q] * g.x, e.y + w[a + q] * g.y);
+                }
+            }
+        if (lane == 0) cluster_rr_serial(G, S, T, k, mat, a, n, w, YB, MU);
+        __syncwarp();
     }
 }
 
@@ -2061,7 +2078,15 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const 
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_cluster");
-    k_ref_cluster_solve<XT><<<gw, 256, 0, st>>>(X, Res, W, CL, YB, MU, n, nb);
+    {
+        const size_t smem_cs = 8 * 3 * RF_KMAX * RF_KMAX * sizeof(cplx);   // 8 warps x (G, S, T)
+        if (cudaFuncSetAttribute(k_ref_cluster_solve<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cs) !=
+            cudaSuccess)
+            return RLMB_ERR_CUDA;
+        // a bounded grid (8 warps per CTA, two CTAs per SM by shared memory) strides over gw warps
+        const unsigned grid = (unsigned)std::min<size_t>(gw, 4 * 2 * 148);
+        k_ref_cluster_solve<XT><<<grid, 256, smem_cs, st>>>(X, Res, W, CL, YB, MU, n, nb);
+    }
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_diag");
     k_ref_diag<<<(unsigned)(((size_t)nb * n + 255) / 256), 256, 0, st>>>(ST, CL, W, F, n, nb);
