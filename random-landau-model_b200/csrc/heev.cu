@@ -1106,7 +1106,7 @@ __global__ void k_z_to_x(const double* __restrict__ Z, C* __restrict__ X, int n,
 }
 
 // ------------------------------------------------------------------ GEMM operands
-// Element accessors for k_zgemm (A: elem(mat, r, k), B: elem(mat, k, c)).
+// Element accessors for the GEMM engines of launch_zgemm (A: elem(mat, r, k), B: elem(mat, k, c)).
 
 // A(r, k) = P(r, k) of a column-major P (entry at p[k*ld + r]): r contiguous.
 template <class C, class PT>
@@ -1249,7 +1249,7 @@ struct EpSub {     // X(r, c) -= acc
 // brought up to date with the panel's earlier pairs, its matrix-vector product reads the
 // leading c x c block as stored (read only) and is corrected by the same pairs.  The
 // rank-2*HP_W update A -= V W^H + W V^H of the remaining leading block then runs as a GEMM
-// over all SMs (k_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
+// over all SMs (launch_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
 // k_hetrd.  D, E, TAU and the reflector storage are those of the unblocked reduction.
 static constexpr int HP_W = 32;      // panel width
 static constexpr int HT_TAIL = 64;   // order below which the unblocked kernel finishes
