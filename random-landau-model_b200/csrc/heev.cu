@@ -1239,6 +1239,13 @@ struct EpSub {     // X(r, c) -= acc
         C* q = x + mat * (size_t)n * n + (size_t)c * n + r;
         *q = csub(*q, acc);
     }
+    // the DMMA engine prefetches X(r, c) into shared memory and passes it back as `old`
+    __device__ __forceinline__ const C* pre_src(size_t mat, int r, int c) const {
+        return x + mat * (size_t)n * n + (size_t)c * n + r;
+    }
+    __device__ __forceinline__ void store_pre(size_t mat, int r, int c, C acc, C old) const {
+        x[mat * (size_t)n * n + (size_t)c * n + r] = csub(old, acc);
+    }
 };
 
 // ------------------------------------------------------------- blocked k_hetrd (large n)
@@ -1466,6 +1473,15 @@ struct EpHer2k {
         C x = csub(*q, acc);
         if (r == c) x.y = 0;
         *q = x;
+    }
+    // the DMMA engine prefetches A(r, c) (on and above the diagonal) into shared memory
+    __device__ __forceinline__ const C* pre_src(size_t mat, int r, int c) const {
+        return r > c ? nullptr : a + mat * (size_t)n * n + (size_t)c * n + r;
+    }
+    __device__ __forceinline__ void store_pre(size_t mat, int r, int c, C acc, C old) const {
+        C x = csub(old, acc);
+        if (r == c) x.y = 0;
+        a[mat * (size_t)n * n + (size_t)c * n + r] = x;
     }
 };
 

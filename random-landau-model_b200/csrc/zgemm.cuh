@@ -147,6 +147,26 @@ struct ZtTiles {
     cplx b[2][ZG_KC][ZG_BN + ZT_PAD];
 };
 
+// An epilogue that updates C in place may expose pre_src(mat, r, c) (address of C(r, c), or
+// null where it writes nothing) and store_pre(mat, r, c, acc, old).  k_zgemm_dmma then copies
+// each thread's C entries into shared memory with cp.async when it starts, so that the
+// epilogue's reads of C overlap the main loop instead of following it.  Thread t's entry
+// idx sits at slot idx * 256 + t (consecutive threads, consecutive 16-byte words).
+template <class T, class = void>
+struct zg_has_pre : std::false_type {};
+template <class T>
+struct zg_has_pre<T, std::void_t<decltype(&T::pre_src)>> : std::true_type {};
+
+template <int BM, class EP>
+constexpr size_t zgemm_dmma_smem() {
+    return sizeof(ZtTiles<BM>) + (zg_has_pre<EP>::value ? (size_t)256 * 4 * (ZG_BN * (BM / 32) / 64) * 2 * sizeof(cplx) : 0);
+}
+
+__device__ __forceinline__ void zg_cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
     asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
         : "+d"(d[0]), "+d"(d[1])
@@ -168,6 +188,21 @@ k_zgemm_dmma(LA la, LB lb, EP ep, int M, int N, int K) {
     const size_t mat = blockIdx.z;
     const int r0 = blockIdx.x * BM, c0 = blockIdx.y * ZG_BN;
     if (ep.skip(r0, c0, BM)) return;   // output tile not needed (whole CTA leaves together)
+    constexpr bool PRE = zg_has_pre<EP>::value;
+    cplx* pre = reinterpret_cast<cplx*>(zg_smem + sizeof(ZtTiles<BM>));
+    if constexpr (PRE) {
+#pragma unroll
+        for (int i = 0; i < MI; ++i)
+#pragma unroll
+            for (int j = 0; j < NJ; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int r = r0 + 32 * wr + 8 * i + g, c = c0 + WN * wc + 8 * j + 2 * q + e;
+                    const cplx* src = (r < M && c < N) ? ep.pre_src(mat, r, c) : nullptr;
+                    if (src) zg_cp_async16(pre + ((i * NJ + j) * 2 + e) * 256 + t, src);
+                }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
     cplx fa[EA], fb[EB];
     auto a_pos = [&](int e, int& kk, int& rr) {
         const int idx = t + 256 * e;
@@ -253,6 +288,7 @@ k_zgemm_dmma(LA la, LB lb, EP ep, int M, int N, int K) {
         if (more) put(cur ^ 1);
         __syncthreads();
     }
+    if constexpr (PRE) asm volatile("cp.async.wait_group 0;\n" ::: "memory");   // this thread's own copies
 #pragma unroll
     for (int i = 0; i < MI; ++i) {
         const int r = r0 + 32 * wr + 8 * i + g;
@@ -262,7 +298,13 @@ k_zgemm_dmma(LA la, LB lb, EP ep, int M, int N, int K) {
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int c = c0 + WN * wc + 8 * j + 2 * q + e;
-                if (c < N) ep.store(mat, r, c, mk(cr[i][j][e], ci[i][j][e]));
+                if (c >= N) continue;
+                if constexpr (PRE) {
+                    if (ep.pre_src(mat, r, c))
+                        ep.store_pre(mat, r, c, mk(cr[i][j][e], ci[i][j][e]), pre[((i * NJ + j) * 2 + e) * 256 + t]);
+                } else {
+                    ep.store(mat, r, c, mk(cr[i][j][e], ci[i][j][e]));
+                }
             }
     }
 }
@@ -274,7 +316,7 @@ cudaError_t launch_zgemm(cudaStream_t st, const LA& la, const LB& lb, const EP& 
     const dim3 grid((M + BM - 1) / BM, (N + ZG_BN - 1) / ZG_BN, nb);
     if constexpr (std::is_same<C, cplx>::value) {
         auto kern = k_zgemm_dmma<BM, LA, LB, EP>;
-        const size_t smem = sizeof(ZtTiles<BM>);
+        const size_t smem = zgemm_dmma_smem<BM, EP>();
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         kern<<<grid, 256, smem, st>>>(la, lb, ep, M, N, K);
