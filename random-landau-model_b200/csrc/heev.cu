@@ -404,7 +404,7 @@ __device__ __forceinline__ int sturm_poly(const double* __restrict__ d, const do
         if (big > 0x1p+400 || big < 0x1p-400) {
             int ex;
             frexp(big, &ex);
-            const double sc = ldexp(1.0, -ex);
+            const double sc = ldexp(1.0, min(max(-ex, -1000), 1000));   // a denormal pair: no overflow
             p *= sc;
             pm *= sc;
             dp *= sc;
@@ -438,14 +438,14 @@ __device__ __forceinline__ void sturm_count2(const double* __restrict__ d, const
         if (biga > 0x1p+400 || biga < 0x1p-400) {
             int ex;
             frexp(biga, &ex);
-            const double sc = ldexp(1.0, -ex);
+            const double sc = ldexp(1.0, min(max(-ex, -1000), 1000));   // a denormal pair: no overflow
             pa *= sc;
             pma *= sc;
         }
         if (bigb > 0x1p+400 || bigb < 0x1p-400) {
             int ex;
             frexp(bigb, &ex);
-            const double sc = ldexp(1.0, -ex);
+            const double sc = ldexp(1.0, min(max(-ex, -1000), 1000));   // a denormal pair: no overflow
             pb *= sc;
             pmb *= sc;
         }
@@ -594,8 +594,10 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
         if (tid == 0 && info) info[mat] = 0;
         return;
     }
-    // ---- eigenvalue k: bisection on Sturm counts, accelerated by safeguarded Newton steps
-    //      on det(T - x I) once the bracket holds k alone (dstebz bracketing, restated)
+    // ---- eigenvalue k: bisection on Sturm counts (dstebz bracketing, restated), accelerated
+    //      by safeguarded Newton steps on det(T - x I), taken from the current point or from
+    //      either end of the bracket, with the step scaled by the number m of eigenvalues in
+    //      the bracket (exact for an m-fold root)
     if (PHASE == 1) {
     const double atol = 2.0 * DBL_EPSILON * onenrm;
     // one collective pass first: Sturm counts at the TRI_THREADS+1 equally spaced points of
@@ -623,38 +625,60 @@ k_tridiag(const double* __restrict__ D, const double* __restrict__ E, double* __
             if (cell + step < TRI_THREADS && s_gc[cell + step] <= k) cell += step;
         double lo = s_gx[cell], hi = s_gx[cell + 1];
         int clo = s_gc[cell], chi = s_gc[cell + 1];
+        // Newton steps p/p' recorded at the bracket ends (valid flags), bracket widths of the
+        // last two steps (bisection is forced when the bracket did not halve over two steps)
+        double rlo = 0.0, rhi = 0.0;
+        bool vlo = false, vhi = false;
+        double w1 = hi - lo, w2 = hi - lo;
         double x = 0.5 * (lo + hi);
         double res = x;
-        bool done = false;
         for (int it = 0; it < 200; ++it) {
             double ratio;
             const int c = sturm_poly(d, e2, n, x, pivmin, ratio);
-            if (c > k) { hi = x; chi = c; } else { lo = x; clo = c; }
+            const bool rok = isfinite(ratio);
+            if (c > k) { hi = x; chi = c; rhi = ratio; vhi = rok; } else { lo = x; clo = c; rlo = ratio; vlo = rok; }
             const double tol = fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
-            if (hi - lo <= tol) { res = 0.5 * (lo + hi); done = true; break; }
+            if (hi - lo <= tol) { res = 0.5 * (lo + hi); break; }
             double xn = 0.5 * (lo + hi);
-            if (chi - clo == 1 && (it % 4) != 3 && isfinite(ratio)) {
-                const double nt = x - ratio;
-                if (nt > lo && nt < hi) {
-                    if (fabs(nt - x) <= tol) {
-                        // converged step: accept only if Sturm counts bracket index k at nt +- 2 tol
-                        const double a0 = fmax(lo, nt - 2.0 * tol), b0 = fmin(hi, nt + 2.0 * tol);
-                        int ca, cb;
-                        sturm_count2(d, e2, n, a0, b0, pivmin, ca, cb);
-                        if (ca <= k && cb > k) { res = nt; done = true; break; }
-                        if (ca > k) { hi = a0; chi = ca; } else { lo = a0; clo = ca; }
-                        if (cb > k) { hi = fmin(hi, b0); chi = cb; } else { lo = fmax(lo, b0); clo = cb; }
-                        xn = 0.5 * (lo + hi);
-                    } else {
-                        xn = nt;
-                    }
+            // Newton candidates x - m p/p' from x and from the two bracket ends, m = eigenvalues
+            // in the bracket (the modified step converges on an m-fold cluster); the smallest
+            // step first: a step within tol is verified by paired counts, else the first
+            // candidate inside the bracket is taken
+            const double m = (double)(chi - clo);
+            double cs[3], cn[3];
+            int nc = 0;
+            if (rok) { cs[nc] = fabs(m * ratio); cn[nc++] = x - m * ratio; }
+            if (vlo && x != lo) { cs[nc] = fabs(m * rlo); cn[nc++] = lo - m * rlo; }
+            if (vhi && x != hi) { cs[nc] = fabs(m * rhi); cn[nc++] = hi - m * rhi; }
+            for (int i = 1; i < nc; ++i)
+                for (int j = i; j > 0 && cs[j] < cs[j - 1]; --j) {
+                    const double ts = cs[j], tn = cn[j];
+                    cs[j] = cs[j - 1]; cn[j] = cn[j - 1];
+                    cs[j - 1] = ts; cn[j - 1] = tn;
                 }
+            bool accepted = false;
+            for (int ci = 0; ci < nc; ++ci) {
+                const double nt = cn[ci];
+                if (cs[ci] <= tol) {
+                    // converged step: accept only if Sturm counts bracket index k at nt +- 2 tol
+                    const double a0 = fmax(lo, nt - 2.0 * tol), b0 = fmin(hi, nt + 2.0 * tol);
+                    int ca, cb;
+                    sturm_count2(d, e2, n, a0, b0, pivmin, ca, cb);
+                    if (ca <= k && cb > k) { res = fmin(fmax(nt, lo), hi); accepted = true; break; }
+                    if (ca > k) { hi = a0; chi = ca; vhi = false; } else { lo = b0; clo = cb; vlo = false; }
+                    xn = 0.5 * (lo + hi);
+                    break;
+                }
+                if (nt > lo && nt < hi) { xn = nt; break; }
             }
-            if (xn <= lo || xn >= hi) { res = 0.5 * (lo + hi); done = true; break; }
+            if (accepted) break;
+            if (hi - lo > 0.5 * w2) xn = 0.5 * (lo + hi);
+            w2 = w1;
+            w1 = hi - lo;
+            if (xn <= lo || xn >= hi) { res = 0.5 * (lo + hi); break; }
             x = xn;
             res = x;
         }
-        (void)done;
         W[mat * n + k] = res;
     }
     return;
