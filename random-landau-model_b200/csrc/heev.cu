@@ -474,26 +474,29 @@ __device__ void twisted_vector(const double* __restrict__ d, const double* __res
                                const double* __restrict__ e2, int n, double x, double pivmin,
                                double* __restrict__ z, int k, double* __restrict__ dplus,
                                double* __restrict__ dminus, int sc) {
+    // D+ (forward, stationary) and D- (backward, progressive) are independent division
+    // chains: one loop advances both, j forward and n-1-j backward
     double q = d[0] - x;
     if (fabs(q) <= pivmin) q = -pivmin;
     dplus[sc] = q;
+    double qb = d[n - 1] - x;
+    if (fabs(qb) <= pivmin) qb = -pivmin;
+    dminus[(size_t)(n - 1) * TRI_THREADS + sc] = qb;
     for (int j = 1; j < n; ++j) {
         q = d[j] - x - e2[j - 1] / q;
         if (fabs(q) <= pivmin) q = -pivmin;
         dplus[(size_t)j * TRI_THREADS + sc] = q;
-    }
-    double qb = d[n - 1] - x;
-    if (fabs(qb) <= pivmin) qb = -pivmin;
-    dminus[(size_t)(n - 1) * TRI_THREADS + sc] = qb;
-    int r = n - 1;
-    double gbest = fabs(q);   // gamma_{n-1} = D+_{n-1}
-    for (int j = n - 2; j >= 0; --j) {
-        const double aj = d[j] - x;
-        double qn = aj - e2[j] / qb;
+        const int jb = n - 1 - j;
+        double qn = (d[jb] - x) - e2[jb] / qb;
         if (fabs(qn) <= pivmin) qn = -pivmin;
         qb = qn;
-        dminus[(size_t)j * TRI_THREADS + sc] = qb;
-        const double gam = fabs(dplus[(size_t)j * TRI_THREADS + sc] + qb - aj);
+        dminus[(size_t)jb * TRI_THREADS + sc] = qb;
+    }
+    // twist index r = argmin |gamma_j|, gamma_j = D+_j + D-_j - (d_j - x), gamma_{n-1} = D+_{n-1}
+    int r = n - 1;
+    double gbest = fabs(q);
+    for (int j = n - 2; j >= 0; --j) {
+        const double gam = fabs(dplus[(size_t)j * TRI_THREADS + sc] + dminus[(size_t)j * TRI_THREADS + sc] - (d[j] - x));
         if (gam < gbest) {
             gbest = gam;
             r = j;
