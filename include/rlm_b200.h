@@ -90,7 +90,7 @@ int rlmb_heevd_host(rlmb_context* ctx, double* h_a, double* h_w, int n, int batc
  * context, work is queued on `stream` (a cudaStream_t, 0 = legacy default stream).
  * Scratch is a fixed file-scope device array of RLMB_NOALLOC_SCRATCH_BYTES that every GPU
  * loading the library holds until exit; a matrix order whose scratch does not fit
- * (n > 919) returns RLMB_ERR_TOO_LARGE, larger batches are processed in chunks.  The first
+ * (n > 927) returns RLMB_ERR_TOO_LARGE, larger batches are processed in chunks.  The first
  * call on each device looks the array's device address up (cudaGetSymbolAddress), so make
  * that first call before any stream capture.  All calls share the array: calls whose GPU
  * work overlaps in time (other streams or host threads) race. */

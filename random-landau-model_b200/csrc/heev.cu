@@ -5,8 +5,8 @@
 // and magma_diag_hamil (diag_wrappers/magma_diag.cu:2-49).  The LAPACK arithmetic those
 // calls reach is restated from its published algorithms:
 //
-//   reduction      A = Q T Q^H (zhetrd, uplo='U').  From order 256: panels of 32 columns
-//                  (k_hetrd_panel, zlatrd restated, one CTA per matrix) whose rank-64
+//   reduction      A = Q T Q^H (zhetrd, uplo='U').  From order 256: panels of 16 columns
+//                  (k_hetrd_panel, zlatrd restated, one CTA per matrix) whose rank-32
 //                  updates run as batched GEMMs over all SMs (launch_zgemm); the last leading
 //                  block (order <= 64, or all of a smaller matrix) by the unblocked,
 //                  look-ahead k_hetrd (zhetd2), its triangle resident in shared memory.
@@ -1285,7 +1285,7 @@ struct EpSub {     // X(r, c) -= acc
 // rank-2*HP_W update A -= V W^H + W V^H of the remaining leading block then runs as a GEMM
 // over all SMs (launch_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
 // k_hetrd.  D, E, TAU and the reflector storage are those of the unblocked reduction.
-static constexpr int HP_W = 32;      // panel width
+static constexpr int HP_W = 16;      // panel width (16 measured faster than 8, 12, 24 and 32 at orders 256-1000)
 static constexpr int HT_TAIL = 64;   // order below which the unblocked kernel finishes
 static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
 

@@ -75,7 +75,7 @@ def test_noalloc_rejects_orders_beyond_its_scratch():
         pytest.skip("no CUDA device")
     import rlmb
     lib = rlmb.lib()
-    n = 920
+    n = 928
     a = torch.zeros((1, n, n), dtype=torch.complex128, device="cuda")
     w = torch.zeros((1, n), dtype=torch.float64, device="cuda")
     rc = lib.rlmb_heevd_batched_noalloc(ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(w.data_ptr()), n, 1,
