@@ -53,6 +53,19 @@ def test_argument_errors_are_reported_not_crashing():
     assert lib.rlmb_rlm_mesh_solve(None, 16, 1.0, 16.0, 4, 1, 0, 1, None, None) == -1
 
 
+def test_noalloc_order_limit_checked_on_the_host():
+    """rlmb_heevd_batched_noalloc sizes its scratch on the host before any CUDA call: orders up
+    to 927 fit its 32 MiB array (an empty batch returns at once), 928 does not.  The device
+    pointers are placeholders that are never dereferenced."""
+    lib = rlmb.lib()
+    fake = ctypes.c_void_p(256)
+    assert lib.rlmb_heevd_batched_noalloc(fake, fake, 927, 0, None, None) == 0
+    rc = lib.rlmb_heevd_batched_noalloc(fake, fake, 928, 1, None, None)
+    assert rc == -5
+    assert b"scratch limit" in lib.rlmb_status_string(rc)
+    assert lib.rlmb_heevd_batched_noalloc(None, fake, 16, 1, None, None) == -1
+
+
 @pytest.mark.parametrize("name", ["rlm_n16_g64_c2_s1.npz", "rlm_n16_g8_c2_s1.npz",
                                   "rlm_n32_g4_c1_s7.npz", "rlm_n64_g4_c1_s3.npz",
                                   "rlm_n128_g2_c1_s5.npz"])
