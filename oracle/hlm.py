@@ -15,7 +15,7 @@ from .fhs import line_chern
 
 
 class HlmParams:
-    """hlm/main_hlm_cpu.cpp:306-309."""
+    """hlm/main_hlm_cpu.cpp:28-30."""
 
     def __init__(self, lx=3, ly=3, Q=3, band=0, n_mesh=32, n_sample=1, seed=1):
         self.lx, self.ly, self.Q, self.band = int(lx), int(ly), int(Q), int(band)
@@ -77,7 +77,7 @@ def solve_kpoint(p: HlmParams, potential, theta_1, theta_2, basis=None):
 
 
 def run_sample(p: HlmParams, potential, keep=False):
-    """hlm/main_hlm_cpu.cpp:354-475 for one sample's potential.
+    """hlm/main_hlm_cpu.cpp:75-197 for one sample's potential.
     theta_2 runs over [0, g) per line; slot g is the periodic copy of slot 0 (:396-397,
     :428-429); energies add theta_2 = 0 twice (:390-394); Chern = sum of +arg/2pi
     (:463-466).  Returns energies [N], chern [N], energies_mesh [(g+1), g, N]."""

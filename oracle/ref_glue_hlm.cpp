@@ -23,9 +23,9 @@ void ref_hlm_wfs_ktheta(int lx, int ly, int Q, int band, int n_mesh, int theta_1
 }
 
 // One theta_1 line (theta_2 = 0..n_mesh-1) of projection + heevd + back-transform,
-// dealt over threads as hlm/main_hlm_cpu.cpp:333-336,363-382 does.  wfs_full is the
+// dealt over threads as hlm/main_hlm_cpu.cpp:55-57,84-103 does.  wfs_full is the
 // 2-line ring, 2*(n_mesh+1)*n_phi*n_sites values; energy_theta is (n_mesh+1)*n_phi.
-// Also applies the periodic copy theta_2=n_mesh <- theta_2=0 of hlm/main_hlm_cpu.cpp:396-397,428-429.
+// Also applies the periodic copy theta_2=n_mesh <- theta_2=0 of hlm/main_hlm_cpu.cpp:117-118,149-150.
 void ref_hlm_solve_line(int theta_1, int lx, int ly, int Q, int band, int n_mesh,
                         std::complex<double>* wfs_full, double* energy_theta, double* potential,
                         int num_threads) {
@@ -61,7 +61,7 @@ void ref_hlm_solve_line(int theta_1, int lx, int ly, int Q, int band, int n_mesh
             wfs_full[((theta_1 % 2) * (n_mesh + 1)) * dim_wfs + k];
 }
 
-// diag_wrappers/chern.cpp:37-75 over threads (hlm/main_hlm_cpu.cpp:434-447).
+// diag_wrappers/chern.cpp:37-75 over threads (hlm/main_hlm_cpu.cpp:155-168).
 void ref_peer_cal_chern(std::complex<double>* wave_functions, double* chern_theta, int n_phi,
                         int dim_vec, int n_mesh, int theta_1, int num_threads) {
     std::vector<std::vector<int>> lists(num_threads);
@@ -82,7 +82,7 @@ void ref_peer_cal_chern(std::complex<double>* wave_functions, double* chern_thet
     for (int id = 0; id < num_threads; ++id) pthread_join(th[id], NULL);
 }
 
-// hlm/main_hlm_cpu.cpp:345-358: the run-long MT19937 stream, one n_sites draw per sample.
+// hlm/main_hlm_cpu.cpp:66-67,79: the run-long MT19937 stream, one n_sites draw per sample.
 void ref_hlm_potentials(unsigned long seed, int n_sites, int n_sample, double* out) {
     VSLStreamStatePtr s;
     vslNewStream(&s, VSL_BRNG_MT19937, seed);

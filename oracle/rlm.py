@@ -108,6 +108,36 @@ def assemble(p: RlmParams, v_mn, coeff_m_theta, coeff_jm, theta_1, theta_2):
     return buf.reshape(-1)
 
 
+def gpu_potential_coeff(x, y, s, coeff_mn, dim, off_head):
+    """rlm/potential_coeff.cu:3-19, the single-precision GPU driver's V_mn (evaluated here in
+    double): V[m,n] = coeff_mn * sum_i s_i e^{+i(kx x_i + ky y_i)} -- the opposite phase sign
+    of the CPU path's get_potential_coeff."""
+    return np.conj(potential_coeff(x, y, s, np.ones_like(coeff_mn), dim, off_head)) * coeff_mn
+
+
+def gpu_assemble(ct1, ct2, coeff_jm, v_mn, N, o):
+    """rlm/hamiltonian_rlm_gpu.cu:9-41, the GPU driver's row-major buffer (in double):
+    H[j][k] (k >= j) = sum_m c_jm[j,m] ct2[m] * sum_{n in {o+k-j, o+k-j-N}} V[m,n] conj(ct1[n]),
+    lower triangle = conj(upper), diagonal stored conjugated.  ct1 / ct2 are the coeff_m_theta
+    rows of theta_1 / theta_2 (rlm/main_rlm_gpu.cu:170-173)."""
+    d = 2 * o + 1
+    V = np.asarray(v_mn).reshape(d, d)
+    G = V * np.conj(ct1)[None, :]
+    T = np.zeros((d, N), dtype=np.complex128)
+    for delta in range(N):
+        if delta <= o:
+            T[:, delta] += G[:, o + delta]
+        if N - delta <= o:
+            T[:, delta] += G[:, o + delta - N]
+    P = np.asarray(ct2)[None, :] * np.asarray(coeff_jm).reshape(N, d)
+    R = P @ T
+    jj, kk = np.triu_indices(N)
+    buf = np.zeros((N, N), dtype=np.complex128)
+    buf[jj, kk] = R[jj, kk - jj]
+    buf[kk, jj] = np.conj(buf[jj, kk])
+    return buf.reshape(-1)
+
+
 def heevd(buf, n):
     """diag_wrappers/mkl_diag.cpp:2-9: column-major, uplo='U', jobz='V', in place.
     Returns (eigenvalues ascending, buffer with eigenvector n at buf[n*N:(n+1)*N])."""

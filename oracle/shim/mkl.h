@@ -10,7 +10,7 @@
  * `scipy_`-prefixed exports of the OpenBLAS that ships inside scipy
  * (LAPACKE_zheevd/cheevd, cblas_zgemm3m/cgemm3m, cblas_zdotc_sub/cdotc_sub).
  * The VSL random-number subset used by rlm/disorder_potential.cpp:3-21 and
- * hlm/main_hlm_cpu.cpp:345-358 is implemented here from the published MT19937
+ * hlm/main_hlm_cpu.cpp:66-67,79 is implemented here from the published MT19937
  * algorithm (Matsumoto & Nishimura, ACM TOMACS 8(1), 1998):
  *   - vslNewStream(MT19937, seed): state seeded with init_genrand(seed mod 2^32);
  *   - vslSkipAheadStream(n): discards n 32-bit outputs;
@@ -19,7 +19,7 @@
  *     u = a + (b - a) * (x * 2^-32).
  * MKL's exact integer->double mapping is not part of the reference tree, so this
  * generator pins "same seed -> same disorder" inside this repository only.  The
- * product's host generator (random-landau-model_b200/csrc/host/disorder.cpp)
+ * product's host generator (random-landau-model_b200/csrc/host_tables.cpp)
  * implements the same published algorithm and mapping independently.
  */
 #ifndef RLMB_ORACLE_MKL_SHIM_H

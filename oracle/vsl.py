@@ -88,7 +88,7 @@ def rlm_disorder(impurity_num: int, L1: float, L2: float, seed: int, sample: int
 
 
 def hlm_potentials(seed: int, n_sites: int, n_sample: int) -> np.ndarray:
-    """hlm/main_hlm_cpu.cpp:345-358: one run-long stream, n_sites draws in [-1,1) per sample."""
+    """hlm/main_hlm_cpu.cpp:66-67,79: one run-long stream, n_sites draws in [-1,1) per sample."""
     s = MT19937(seed)
     return np.stack([s.uniform(n_sites, -1.0, 1.0) for _ in range(n_sample)]) if n_sample else \
         np.zeros((0, n_sites))

@@ -89,7 +89,111 @@ int chern_line(const std::complex<double>* wfs_full, double* chern_theta, int n_
     return rc;
 }
 
+// H(theta_1, theta_2) of the reference's single-precision GPU driver
+// (rlm/hamiltonian_rlm_gpu.cu:9-41): row-major wfs[j*n + k] for k >= j is
+//   sum_m coeff_jm[j*d + m] ct2[m] sum_{n: (n - o) = k - j mod N, |n - o| <= o} Vmn[m*d + n] conj(ct1[n]),
+// the lower triangle its conjugate and the diagonal conjugated (the reference's last store
+// at wfs[k*n + j] overwrites the diagonal with its conjugate).  Products and sums in double,
+// rounded to float once.  One thread per (j, k); k < j threads return, so every entry is
+// written exactly once (the reference zeroes the lower triangle from one thread while
+// another writes it; this writes the full Hermitian matrix it intends).
+__global__ void k_set_hamil_f32(const cuFloatComplex* __restrict__ ct1, const cuFloatComplex* __restrict__ ct2,
+                                const cuFloatComplex* __restrict__ cjm, const cuFloatComplex* __restrict__ vmn,
+                                cuFloatComplex* __restrict__ wfs, int N, int d, int o) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= N || k >= N || k < j) return;
+    // the (at most two) n of the cyclic band: n - o = k - j, or k - j - N
+    int nn[2], cnt = 0;
+    if (k - j <= o) nn[cnt++] = o + k - j;
+    if (N + j - k <= o) nn[cnt++] = o + k - j - N;
+    double hr = 0.0, hi = 0.0;
+    if (cnt > 0) {
+        double tr[2], ti[2];   // conj(ct1[n])
+        for (int q = 0; q < cnt; ++q) {
+            tr[q] = ct1[nn[q]].x;
+            ti[q] = -ct1[nn[q]].y;
+        }
+        for (int m = 0; m < d; ++m) {
+            double sr = 0.0, si = 0.0;
+            for (int q = 0; q < cnt; ++q) {
+                const cuFloatComplex v = vmn[(size_t)m * d + nn[q]];
+                sr += v.x * tr[q] - v.y * ti[q];
+                si += v.x * ti[q] + v.y * tr[q];
+            }
+            const cuFloatComplex a = cjm[(size_t)j * d + m], b = ct2[m];
+            const double pr = sr * a.x - si * a.y, pi = sr * a.y + si * a.x;
+            hr += pr * b.x - pi * b.y;
+            hi += pr * b.y + pi * b.x;
+        }
+    }
+    const cuFloatComplex h = make_cuFloatComplex((float)hr, (float)hi);
+    const cuFloatComplex hc = make_cuFloatComplex((float)hr, (float)-hi);
+    if (j == k) {
+        wfs[(size_t)j * N + j] = hc;
+    } else {
+        wfs[(size_t)j * N + k] = h;
+        wfs[(size_t)k * N + j] = hc;
+    }
+}
+
+// V_mn of the reference's single-precision GPU path (rlm/potential_coeff.cu:3-19):
+//   Vmn[m*dim_n + n] = coeff_mn[m*dim_n + n] * sum_i s_i exp(+i 2 pi ((m - o) x_i + (n - o) y_i))
+// (the GPU path's sign; its CPU path uses exp(-i ...)).  One warp per (m, n), lanes over the
+// impurities, phases and sums in double, rounded to float once.
+__global__ void k_potential_f32(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ s,
+                                cuFloatComplex* __restrict__ vmn, const cuFloatComplex* __restrict__ cmn, int dim_m,
+                                int dim_n, int o, int nimp) {
+    const int lane = threadIdx.x & 31;
+    const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= (long)dim_m * dim_n) return;
+    const int m = (int)(w / dim_n), n = (int)(w % dim_n);
+    const double km = 2.0 * (m - o), kn = 2.0 * (n - o);
+    double sr = 0.0, si = 0.0;
+    for (int i = lane; i < nimp; i += 32) {
+        double sn, cs;
+        sincospi(km * (double)x[i] + kn * (double)y[i], &sn, &cs);
+        sr += cs * (double)s[i];
+        si += sn * (double)s[i];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
+    }
+    if (lane == 0) {
+        const cuFloatComplex c = cmn[(size_t)m * dim_n + n];
+        vmn[(size_t)m * dim_n + n] = make_cuFloatComplex((float)(sr * c.x - si * c.y), (float)(sr * c.y + si * c.x));
+    }
+}
+
 }  // namespace
+
+void set_hamil_matrix(const cuFloatComplex* dev_coeff_m_theta_1, const cuFloatComplex* dev_coeff_m_theta_2,
+                      const cuFloatComplex* dev_coeff_jm, const cuFloatComplex* dev_Vmn, cuFloatComplex* dev_wfs,
+                      int n_phi, int dim_n, int off_head) {
+    if (!dev_coeff_m_theta_1 || !dev_coeff_m_theta_2 || !dev_coeff_jm || !dev_Vmn || !dev_wfs || n_phi <= 0 ||
+        dim_n != 2 * off_head + 1 || off_head < 0)
+        return report("set_hamil_matrix", RLMB_ERR_ARG);
+    const dim3 block(32, 8), grid((n_phi + 31) / 32, (n_phi + 7) / 8);
+    k_set_hamil_f32<<<grid, block, 0, 0>>>(dev_coeff_m_theta_1, dev_coeff_m_theta_2, dev_coeff_jm, dev_Vmn, dev_wfs,
+                                           n_phi, dim_n, off_head);
+    int rc = cudaGetLastError() == cudaSuccess ? RLMB_OK : RLMB_ERR_CUDA;
+    if (rc == RLMB_OK && cudaStreamSynchronize(0) != cudaSuccess) rc = RLMB_ERR_CUDA;
+    report("set_hamil_matrix", rc);
+}
+
+void prepare_potential_coeff(float* impurity_x, float* impurity_y, float* impurity_intensity, cuFloatComplex* Vmn,
+                             cuFloatComplex* coeff_mn, int dim_m, int dim_n, int off_head, int impurity_num) {
+    if (!impurity_x || !impurity_y || !impurity_intensity || !Vmn || !coeff_mn || dim_m <= 0 || dim_n <= 0 ||
+        impurity_num < 0)
+        return report("prepare_potential_coeff", RLMB_ERR_ARG);
+    const long warps = (long)dim_m * dim_n;
+    k_potential_f32<<<(unsigned)((warps + 7) / 8), 256, 0, 0>>>(impurity_x, impurity_y, impurity_intensity, Vmn,
+                                                                 coeff_mn, dim_m, dim_n, off_head, impurity_num);
+    int rc = cudaGetLastError() == cudaSuccess ? RLMB_OK : RLMB_ERR_CUDA;
+    if (rc == RLMB_OK && cudaStreamSynchronize(0) != cudaSuccess) rc = RLMB_ERR_CUDA;
+    report("prepare_potential_coeff", rc);
+}
 
 void mkl_heevd(std::complex<double>* hamiltonian, double* energy, int l) {
     rlmb_context* ctx = thread_ctx();
@@ -133,6 +237,23 @@ void magma_diag_hamil(cuFloatComplex* dev_wfs, float* energy, int n_phi) {
 void cal_Chern(std::complex<double>* wfs_full, double* chern_numbers_theta, int n_phi, int dim_vec, int n_mesh,
                int theta_1) {
     report("cal_Chern", chern_line(wfs_full, chern_numbers_theta, n_phi, dim_vec, n_mesh, theta_1));
+}
+
+// diag_wrappers/chern.cpp:77-123: the plaquettes of line theta_1 from the eigenvector files
+// wfs_<slot>_<theta_2>.bin (slot = theta_1 % 2 ring index, theta_2 = 0..n_mesh, as the GPU
+// driver writes them with -DwfsIO).  The reference multiplies <u_{l+1}|u_l> around each
+// plaquette and stores +arg/2pi; that is the conjugate product of cal_Chern's, so the values
+// are cal_Chern's -arg/2pi of the same ring (atan2 is odd in its first argument, signed
+// zeros included).  All 2 (n_mesh + 1) files are read, then the ring goes through cal_Chern.
+void cal_Chern_wfs_IO(double* chern_numbers_theta, int n_phi, int dim_vec, int n_mesh, int theta_1) {
+    if (!chern_numbers_theta || n_phi <= 0 || dim_vec <= 0 || n_mesh <= 0 || theta_1 < 0)
+        return report("cal_Chern_wfs_IO", RLMB_ERR_ARG);
+    const size_t dim_wfs = (size_t)n_phi * dim_vec;
+    std::vector<std::complex<double>> ring(2 * (size_t)(n_mesh + 1) * dim_wfs);
+    for (int slot = 0; slot < 2; ++slot)
+        for (int t2 = 0; t2 <= n_mesh; ++t2)
+            read_wfs(slot, t2, ring.data() + ((size_t)slot * (n_mesh + 1) + t2) * dim_wfs, dim_wfs);
+    report("cal_Chern_wfs_IO", chern_line(ring.data(), chern_numbers_theta, n_phi, dim_vec, n_mesh, theta_1));
 }
 
 void* peer_cal_Chern(void* peer_Chern_params) {

@@ -91,7 +91,7 @@ k_rlm_disorder(uint32_t seed, int nimp, double L1, double L2, int sample0, doubl
     }
 }
 
-// hlm on-site potentials (hlm/main_hlm_cpu.cpp:345-358): one stream for the whole run,
+// hlm on-site potentials (hlm/main_hlm_cpu.cpp:66-67,79): one stream for the whole run,
 // sample k uses outputs [k*n_sites, (k+1)*n_sites), each U[-1,1).  Output [sample][site].
 __global__ void __launch_bounds__(256)
 k_hlm_potentials(uint32_t seed, int n_sites, int sample0, double* __restrict__ out) {

@@ -104,7 +104,7 @@ extern "C" int rlmb_rlm_disorder(int impurity_num, double L1, double L2, unsigne
 
 extern "C" int rlmb_hlm_potentials(unsigned long seed, int n_sites, int n_sample, double* out) {
     if (n_sites <= 0 || n_sample < 0 || (!out && n_sample > 0)) return RLMB_ERR_ARG;
-    // hlm/main_hlm_cpu.cpp:345-358: one stream for the whole run
+    // hlm/main_hlm_cpu.cpp:66-67,79: one stream for the whole run
     Mt19937 g((uint32_t)seed);
     for (long long k = 0; k < (long long)n_sample * n_sites; ++k) out[k] = g.uniform(-1.0, 1.0);
     return RLMB_OK;

@@ -194,7 +194,7 @@ int launch_rlm_links(rlmb_context* ctx, const cplx* X, int n_phi, int g, int nsa
 }
 
 // Plaquette phases and sample accumulation (rlm/main_rlm_cpu.cpp:155-158,187-190,230-239;
-// hlm/main_hlm_cpu.cpp:390-394,422-426,463-470; diag_wrappers/chern.cpp:47-72).
+// hlm/main_hlm_cpu.cpp:111-115,143-147,184-187; diag_wrappers/chern.cpp:47-72).
 // Mesh arrays are [sample][t1 (g+1)][t2 (n2)][N]; for hlm n2 = g and slot g of a line is
 // the periodic copy of slot 0.  Plaquette (line L = 1..g, m = 0..g-1):
 //   prod = U1(L-1,m) * U2(L,m) * conj(U1(L-1,m+1)) * conj(U2(L-1,m))
@@ -468,7 +468,7 @@ int launch_hlm_project(rlmb_context* ctx, const cplx* hb, const cplx* vt, const 
 // theta_1 links (same t2) couple equal ky only,
 //   S[(kx,ky),(kx',ky)] = ly D_Lx'(kx - kx' + (t1 - t1')/g) <hhat|hhat'>,
 // with D_L(s) = sum_{j<L} e^{i 2pi s j / L}.  The theta_2 = g neighbour is the periodic
-// copy of theta_2 = 0 (hlm/main_hlm_cpu.cpp:428-429).
+// copy of theta_2 = 0 (hlm/main_hlm_cpu.cpp:149-150).
 // blockIdx.x = state chunk, blockIdx.y = sample*kpts + t (t = t1*g + t2), blockIdx.z = dir.
 static constexpr int LINK_STATES = 16;
 

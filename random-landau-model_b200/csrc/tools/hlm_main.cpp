@@ -1,7 +1,7 @@
 // hlm -- drop-in for the reference's hlm_cpu_dp program on one B200.
 //
 // Options, usage text, log_hlm.txt and energy_Chern_No.txt are those of
-// hlm/init_hlm.cpp:4-94 and hlm/main_hlm_cpu.cpp:338-475 (-h needs an argument, as in the
+// hlm/init_hlm.cpp:4-94 and hlm/main_hlm_cpu.cpp:22-197 (-h needs an argument, as in the
 // reference).  -t is accepted and has no effect.  The stderr report keeps the reference's
 // lines; its per-k-point times are the device times of the batched kernels for sample 0.
 #include <unistd.h>
@@ -65,7 +65,7 @@ int main(int argc, char* argv[]) {
     rlmb_context* ctx = nullptr;
     int rc = rlmb_create(&ctx, 0);
     if (rc) return driver::fail("rlmb_create", rc);
-    // on-site potentials of every sample from the run-long stream (hlm/main_hlm_cpu.cpp:345-358)
+    // on-site potentials of every sample from the run-long stream (hlm/main_hlm_cpu.cpp:66-67,79)
     vector<double> pots((size_t)n_sample * n_sites);
     rc = rlmb_hlm_potentials(seed, n_sites, n_sample, pots.data());
     if (rc) return driver::fail("rlmb_hlm_potentials", rc);
@@ -94,7 +94,7 @@ int main(int argc, char* argv[]) {
             if (rc < 0) return driver::fail("rlmb_hlm_mesh_solve", rc);
         }
     }
-    // energy_Chern_No.txt exactly as hlm/main_hlm_cpu.cpp:473-475 writes it
+    // energy_Chern_No.txt exactly as hlm/main_hlm_cpu.cpp:194-196 writes it
     for (int n = 0; n < n_sample; ++n)
         for (int i = 0; i < n_phi; ++i)
             fchern << setw(8) << n << " " << setw(15) << setprecision(8) << e[(size_t)n * n_phi + i] << " "

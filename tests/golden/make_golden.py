@@ -7,7 +7,7 @@ Run in a container that has the reference sources (it is never run by the tests)
 
 Every number stored here comes from the reference's own double-precision functions,
 compiled unmodified into oracle/_ref/libref_{rlm,hlm}.so and driven in the order of
-rlm/main_rlm_cpu.cpp:109-243 and hlm/main_hlm_cpu.cpp:354-475, or from the
+rlm/main_rlm_cpu.cpp:109-243 and hlm/main_hlm_cpu.cpp:75-197, or from the
 reference's command-line programs oracle/_ref/{rlm,hlm}_cpu_dp (text output, 8
 significant digits).  Seeds and sizes are recorded in each file.
 """
@@ -116,7 +116,7 @@ def rlm_reference(n_phi, qc, ic, g, n_sample, seed, threads=8, keep_kpoints=()):
 
 def hlm_reference(lx, ly, Q, band, g, n_sample, seed, threads=8, keep_basis=(), only=None,
                   keep_mesh=True):
-    """Per-sample loop of hlm/main_hlm_cpu.cpp:354-475 over the reference's functions
+    """Per-sample loop of hlm/main_hlm_cpu.cpp:75-197 over the reference's functions
     (`only`: the subset of sample indices to solve; the potentials stream covers them all)."""
     lib = hlm_lib()
     n_sites = lx * ly

@@ -126,3 +126,68 @@ def test_get_potential_coeff_wrapper(harness, tmp_path):
     _call(harness, "vmn", tmp_path / "i.bin", tmp_path / "v.bin", nimp, dim, o)
     v = np.fromfile(tmp_path / "v.bin", np.complex128)
     assert np.abs(v - d["v_mn"][0]).max() <= 1e-12 * np.abs(d["v_mn"][0]).max()
+
+
+@pytest.mark.gpu
+def test_prepare_potential_coeff_wrapper(harness, tmp_path):
+    """The GPU driver's V_mn (rlm/potential_coeff.cu:3-26) from float device arrays, against
+    the oracle's restatement of that kernel evaluated in double on the same float inputs."""
+    _gpu()
+    from oracle import rlm as orlm
+    d = golden("rlm_n64_g4_c1_s3.npz")
+    nimp, o = int(d["impurity_num"]), int(d["off_head"])
+    dim = 2 * o + 1
+    x, y, s = (d[k][0].astype(np.float32) for k in ("x", "y", "s"))
+    cmn = d["coeff_mn"].astype(np.complex64)
+    np.concatenate([x, y, s, cmn.view(np.float32)]).astype(np.float32).tofile(tmp_path / "i.bin")
+    _call(harness, "vmngpu", tmp_path / "i.bin", tmp_path / "v.bin", nimp, dim, o)
+    v = np.fromfile(tmp_path / "v.bin", np.complex64).astype(np.complex128)
+    ref = orlm.gpu_potential_coeff(x.astype(np.float64), y.astype(np.float64), s.astype(np.float64),
+                                   cmn.astype(np.complex128), dim, o)
+    assert np.abs(v - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_phi,t1,t2", [(64, 1, 3), (30, 0, 2), (17, 4, 4)])
+def test_set_hamil_matrix_wrapper(harness, tmp_path, n_phi, t1, t2):
+    """The GPU driver's assembly (rlm/hamiltonian_rlm_gpu.cu:9-50) on float device tables,
+    including orders that are not multiples of 8 (the reference's launch needs them)."""
+    _gpu()
+    import rlmb
+    from oracle import rlm as orlm
+    prm = rlmb.rlm_params(n_phi)
+    o, dim, g = prm["off_head"], prm["dim"], 4
+    _, cmt, cjm = rlmb.rlm_coeff_tables(n_phi, o, g, prm["L1"], prm["L2"])
+    rng = np.random.default_rng(n_phi)
+    v = (rng.normal(size=dim * dim) + 1j * rng.normal(size=dim * dim)).astype(np.complex64)
+    ct1 = cmt[t1 * dim:(t1 + 1) * dim].astype(np.complex64)
+    ct2 = cmt[t2 * dim:(t2 + 1) * dim].astype(np.complex64)
+    cjm = cjm.astype(np.complex64)
+    np.concatenate([ct1, ct2, cjm, v]).tofile(tmp_path / "i.bin")
+    _call(harness, "sethamil", tmp_path / "i.bin", tmp_path / "h.bin", n_phi, o)
+    h = np.fromfile(tmp_path / "h.bin", np.complex64).astype(np.complex128)
+    ref = orlm.gpu_assemble(ct1.astype(np.complex128), ct2.astype(np.complex128), cjm.astype(np.complex128),
+                            v.astype(np.complex128), n_phi, o)
+    assert np.abs(h - ref).max() <= 1e-6 * np.abs(ref).max()
+    H = h.reshape(n_phi, n_phi)
+    assert np.array_equal(H, np.conj(H.T))      # Hermitian, every entry written
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("t1", [3, 4])
+def test_cal_chern_wfs_io_wrapper(harness, tmp_path, t1):
+    """cal_Chern_wfs_IO (diag_wrappers/chern.cpp:77-123) on eigenvector files in the
+    write_wfs layout, named by ring slot theta_1 % 2, against the oracle's plaquettes."""
+    _gpu()
+    from oracle import fhs, rlm as orlm
+    p = orlm.RlmParams(16, 1.0, 16.0, 8, 1, 1)
+    X = orlm.run_sample(p, 0, keep=True)["eigvecs"]       # [(g+1), (g+1), N, N]
+    g, N = 8, 16
+    for line in (t1 - 1, t1):
+        for t2 in range(g + 1):
+            X[line, t2].astype(np.complex128).tofile(tmp_path / f"wfs_{line % 2}_{t2}.bin")
+    out = tmp_path / "c.bin"
+    _call(harness, "chernio", tmp_path, out, N, N, g, t1)
+    got = np.fromfile(out, np.float64).reshape(N, g)
+    ref = fhs.line_chern(X[t1 - 1], X[t1]).T
+    assert np.abs(got - ref).max() < 1e-10

@@ -10,6 +10,9 @@
 //   wrappers_check tables   out n_phi off_head n_mesh L             prepare_coeff
 //   wrappers_check disorder out n_imp L seed sample                 generate_disorder_potential
 //   wrappers_check vmn      in out n_imp dim off_head               get_potential_coeff
+//   wrappers_check vmngpu   in out n_imp dim off_head               prepare_potential_coeff (device, float)
+//   wrappers_check sethamil in out n_phi off_head                   set_hamil_matrix (device, float)
+//   wrappers_check chernio  dir out n_phi dim_vec n_mesh theta_1    cal_Chern_wfs_IO on files in dir
 #include <cuda_runtime.h>
 
 #include <complex>
@@ -18,6 +21,8 @@
 #include <cstring>
 #include <fstream>
 #include <vector>
+
+#include <unistd.h>
 
 #include "diag_wrappers_b200.h"
 
@@ -111,6 +116,46 @@ int main(int argc, char** argv) {
                             o, nimp);
         std::ofstream f(argv[3], std::ios::binary);
         dump(f, v.data(), v.size());
+    } else if (mode == "vmngpu") {
+        // in: x, y, s (float, n_imp each), coeff_mn (complex float, dim*dim)
+        const int nimp = atoi(argv[4]), dim = atoi(argv[5]), o = atoi(argv[6]);
+        const size_t dd = (size_t)dim * dim;
+        auto xyz = slurp<float>(argv[2], 3 * (size_t)nimp + 2 * dd);
+        float* d = nullptr;
+        cudaMalloc(&d, (3 * (size_t)nimp + 4 * dd) * sizeof(float));
+        cudaMemcpy(d, xyz.data(), (3 * (size_t)nimp + 2 * dd) * sizeof(float), cudaMemcpyHostToDevice);
+        cuFloatComplex* dc = reinterpret_cast<cuFloatComplex*>(d + 3 * (size_t)nimp);
+        cuFloatComplex* dv = dc + dd;
+        prepare_potential_coeff(d, d + nimp, d + 2 * (size_t)nimp, dv, dc, dim, dim, o, nimp);
+        std::vector<cf> v(dd);
+        cudaMemcpy(v.data(), dv, dd * sizeof(cf), cudaMemcpyDeviceToHost);
+        std::ofstream f(argv[3], std::ios::binary);
+        dump(f, v.data(), dd);
+        cudaFree(d);
+    } else if (mode == "sethamil") {
+        // in: ct1 (dim), ct2 (dim), coeff_jm (n_phi*dim), Vmn (dim*dim), complex float
+        const int n_phi = atoi(argv[4]), o = atoi(argv[5]);
+        const int dim = 2 * o + 1;
+        const size_t nin = 2 * (size_t)dim + (size_t)n_phi * dim + (size_t)dim * dim;
+        auto in = slurp<cf>(argv[2], nin);
+        cuFloatComplex* d = nullptr;
+        cudaMalloc(&d, (nin + (size_t)n_phi * n_phi) * sizeof(cf));
+        cudaMemcpy(d, in.data(), nin * sizeof(cf), cudaMemcpyHostToDevice);
+        cuFloatComplex* wfs = d + nin;
+        set_hamil_matrix(d, d + dim, d + 2 * dim, d + 2 * dim + (size_t)n_phi * dim, wfs, n_phi, dim, o);
+        std::vector<cf> h((size_t)n_phi * n_phi);
+        cudaMemcpy(h.data(), wfs, h.size() * sizeof(cf), cudaMemcpyDeviceToHost);
+        std::ofstream f(argv[3], std::ios::binary);
+        dump(f, h.data(), h.size());
+        cudaFree(d);
+    } else if (mode == "chernio") {
+        const int n_phi = atoi(argv[4]), dim_vec = atoi(argv[5]), g = atoi(argv[6]), t1 = atoi(argv[7]);
+        std::vector<double> ct((size_t)g * n_phi, -7.0);
+        const std::string out = argv[3];
+        if (chdir(argv[2]) != 0) return 3;
+        cal_Chern_wfs_IO(ct.data(), n_phi, dim_vec, g, t1);
+        std::ofstream f(out, std::ios::binary);
+        dump(f, ct.data(), ct.size());
     } else {
         return 2;
     }
