@@ -1,21 +1,25 @@
 #!/usr/bin/env python
-"""Throughput of the twist-mesh pipeline on B200: k-point eigensolves/s.
+"""Throughput of the twist-mesh pipeline on B200: k-point eigensolves/s and samples/hour.
 
-Workload (the hlm configuration the metric is quoted on): Hofstadter lattice 48 x 16 sites,
-flux 1/3 (Q=3), projected onto subband 0 (n_phi = 256, so every k-point is a 256 x 256
-complex Hermitian eigenproblem), twist mesh g=32 (theta_1 in [0,32], theta_2 in [0,32):
-1056 k-points per sample), 64 disorder samples per step = 67,584 eigensolves plus the
-projection and the Chern step.  On-site disorder is uniform in [-1,1) from the seeded
-MT19937 stream of the reference's hlm driver (seed 1 + rank).
+Headline workload (the configuration the north-star target is stated on): random Landau-level
+model, n_phi = 3000 (every k-point a 3000 x 3000 complex Hermitian eigenproblem, 144 MB in
+complex128), 48,000 impurities with strengths +-1 at uniform positions (impurity
+concentration 16), K-space cut o = 110, twist mesh g = 4 ((g+1)^2 = 25 k-points per sample),
+8 disorder samples per step = 200 eigensolves plus the V_mn, assembly and Chern steps.  The
+disorder is drawn on the device from the reference's seeded MT19937 stream (seed 1 + rank).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload rlm3000|hlm48x16|rlm512|fss]
 
-value : device-resident inputs, one rlmb_hlm_mesh_solve_device call per step.
-e2e   : the host-buffer C-ABI call rlmb_hlm_mesh_solve (potentials H2D, energies and
-        Chern numbers D2H inside the timed region).
+value : FP64 mode, rlmb_rlm_mesh_solve_device per step (results stay in device memory).
+e2e   : the host-buffer C-ABI call rlmb_rlm_mesh_solve (coefficient tables H2D, energies and
+        Chern numbers D2H inside the timed region), FP64 mode.
+mixed : the mixed-precision mode (tcgen05 tensor-core products, FP64 refinement) on the same
+        samples, with its agreement with the FP64 mode and with the reference fixture.
+extra : the hlm 48x16 configuration (n_phi = 256, g = 32, 64 samples per step).
 --impl reference : the reference's own CPU implementation (oracle/_ref, compiled from the
-        reference sources) on this host's cores, one theta_1 line per step.
-Multi-GPU (torchrun): every rank solves its own 64 samples (weak scaling, no data-path
+        reference sources) on this host's cores, one k-point per step.
+Multi-GPU (torchrun): every rank solves its own samples (weak scaling, no data-path
 collective); the step time is the max over ranks.
 """
 import argparse
@@ -26,7 +30,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 REPO = os.path.dirname(os.path.abspath(__file__))
@@ -37,7 +40,13 @@ for _p in (REPO, PKG):
 
 METRIC = "k-point eigensolves/s & samples/hr, mixed-refined vs FP64 GPU; Chern ints exact"
 UNIT = "k-point eigensolves/s"
-LX, LY, Q, BAND, G, NS, SEED = 48, 16, 3, 0, 32, 64, 1
+SEED = 1
+# headline: rlm n_phi=3000, g=4, 8 samples per step
+RLM_N, RLM_G, RLM_NS = 3000, 4, 8
+RLM_KPTS = (RLM_G + 1) ** 2
+RLM_FIXTURE = os.path.join(REPO, "tests", "golden", "rlm_n3000_g4_c1_s1_full.npz")
+# hlm 48x16 (the extra block and --workload hlm48x16)
+LX, LY, Q, BAND, G, NS = 48, 16, 3, 0, 32, 64
 N_PHI = LX * LY // Q
 N_SITES = LX * LY
 KPTS = (G + 1) * G
@@ -50,6 +59,17 @@ def _config(extra=None):
          "n_phi": N_PHI, "n_mesh": G, "samples_per_step": NS, "solves_per_step": SOLVES_PER_STEP,
          "precision": "fp64 (complex128) eigensolve, FP64 phase accumulation",
          "l2": "working set per step >> 126 MB L2 (each sample's 1056 matrices are 1.1 GB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def _rlm_config(extra=None):
+    c = {"workload": f"rlm n_phi={RLM_N}, 48000 impurities (concentration 16, strengths +-1), K-space cut o=110, "
+                     f"g={RLM_G} ({RLM_KPTS} k-points/sample), {RLM_NS} samples/step, seed {SEED}+rank",
+         "n_phi": RLM_N, "n_mesh": RLM_G, "samples_per_step": RLM_NS, "solves_per_step": RLM_NS * RLM_KPTS,
+         "precision": "fp64 (complex128) eigensolve, FP64 phase accumulation",
+         "l2": "working set per step >> 126 MB L2 (each matrix is 144 MB; a step's 200 matrices are 29 GB)"}
     if extra:
         c.update(extra)
     return c
@@ -149,6 +169,70 @@ def _ref_line_runner(threads):
     return run_line, None
 
 
+def _ref_rlm_runner(threads):
+    """Closure running one k-point of the reference rlm path at n_phi=3000 (assembly + zheevd
+    by the reference's peer_solve_projected) per call, with the BLAS inside zheevd on
+    `threads` threads.  V_mn of sample 0 is computed once at set-up (the reference's
+    get_potential_coeff, single-threaded) and its time is reported separately."""
+    import numpy as np
+    os.environ["OPENBLAS_NUM_THREADS"] = str(threads)   # before the reference's BLAS loads
+    path = os.path.join(REPO, "oracle", "_ref", "libref_rlm.so")
+    if not os.path.exists(path):
+        return None, f"{path} not built (make -C oracle needs the reference sources)", None
+    lib = ctypes.CDLL(path)
+    for fn in ("ref_rlm_prepare_coeff", "ref_rlm_disorder", "ref_rlm_potential", "ref_rlm_solve_list"):
+        getattr(lib, fn).restype = None
+    c_dp = ctypes.POINTER(ctypes.c_double)
+    L = float(np.sqrt(RLM_N * 1.0))
+    nimp = int(16.0 * RLM_N / 1.0)
+    o = int(np.sqrt(nimp) / 2 + 1)
+    d = 2 * o + 1
+    cmn = np.zeros(d * d, np.complex128)
+    cmt = np.zeros((RLM_G + 1) * d, np.complex128)
+    cjm = np.zeros(RLM_N * d, np.complex128)
+    lib.ref_rlm_prepare_coeff(cmn.ctypes.data_as(c_dp), cmt.ctypes.data_as(c_dp), cjm.ctypes.data_as(c_dp),
+                              RLM_N, o, d, d, RLM_G, ctypes.c_double(L), ctypes.c_double(L))
+    x, y, s = (np.zeros(nimp) for _ in range(3))
+    lib.ref_rlm_disorder(x.ctypes.data_as(c_dp), y.ctypes.data_as(c_dp), s.ctypes.data_as(c_dp), nimp,
+                         ctypes.c_double(L), ctypes.c_double(L), ctypes.c_ulong(SEED), 0)
+    vmn = np.zeros(d * d, np.complex128)
+    t0 = time.perf_counter()
+    lib.ref_rlm_potential(x.ctypes.data_as(c_dp), y.ctypes.data_as(c_dp), s.ctypes.data_as(c_dp),
+                          vmn.ctypes.data_as(c_dp), cmn.ctypes.data_as(c_dp), d, d, o, nimp)
+    vmn_s = time.perf_counter() - t0
+    wf = np.zeros(2 * (RLM_G + 1) * RLM_N * RLM_N, np.complex128)
+    et = np.zeros((RLM_G + 1) * RLM_N)
+    state = {"k": 0}
+
+    def run_point():
+        k = state["k"] % RLM_KPTS
+        t1, t2 = k // (RLM_G + 1), k % (RLM_G + 1)
+        lst = (ctypes.c_int * 1)(t2)
+        lib.ref_rlm_solve_list(t1, lst, 1, RLM_N, RLM_G, d, o, wf.ctypes.data_as(c_dp), et.ctypes.data_as(c_dp),
+                               vmn.ctypes.data_as(c_dp), cjm.ctypes.data_as(c_dp), cmt.ctypes.data_as(c_dp), 1)
+        state["k"] += 1
+        return 1
+    return run_point, None, vmn_s
+
+
+def cpu_baseline_rlm(min_seconds=10.0, max_points=4):
+    """The reference's own CPU rlm path at n_phi=3000 timed on this host (bounded sample: a
+    few k-points, each assembly + zheevd with the BLAS on every host thread)."""
+    threads = os.cpu_count() or 1
+    run_point, err, vmn_s = _ref_rlm_runner(threads)
+    if run_point is None:
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": err}
+    solves, t0 = 0, time.perf_counter()
+    while solves < max_points and (time.perf_counter() - t0 < min_seconds or solves < 1):
+        solves += run_point()
+    dt = time.perf_counter() - t0
+    return {"value": solves / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"sample 0 of the rlm n_phi={RLM_N} g={RLM_G} workload: {solves} k-points (assembly + "
+                      f"LAPACKE_zheevd by peer_solve_projected, BLAS on {threads} threads) in {dt:.1f} s; "
+                      f"the per-sample V_mn (get_potential_coeff, one thread) took {vmn_s:.1f} s and is not "
+                      f"in the rate"}
+
+
 def cpu_baseline(min_seconds=10.0, max_lines=G + 1):
     """The reference's own CPU path timed on this host (bounded sample of the workload)."""
     threads = os.cpu_count() or 1
@@ -173,43 +257,52 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    run_line, err = _ref_line_runner(threads)
-    if run_line is None:
+    if args.workload == "hlm48x16":
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+        run_step, err = _ref_line_runner(threads)
+        cfg = _config({"reference_step": f"one theta_1 line ({G} k-point solves + FHS) of sample 0"})
+        sample = f"{args.steps} theta_1 lines of sample 0, {threads} threads"
+        vmn_s = None
+    else:
+        run_step, err, vmn_s = _ref_rlm_runner(threads)
+        cfg = _rlm_config({"reference_step": "one k-point (assembly + zheevd) of sample 0, BLAS on all host "
+                                             "threads"})
+        sample = f"{args.steps} k-points of sample 0, BLAS on {threads} threads"
+    if run_step is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
     for _ in range(args.warmup):
-        run_line()
+        run_step()
     solves, times = 0, []
     for _ in range(args.steps):
         t = time.perf_counter()
-        solves += run_line()
+        solves += run_step()
         times.append(time.perf_counter() - t)
     total = sum(times)
     value = solves / total
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": _config({"reference_step": f"one theta_1 line ({G} k-point solves + FHS) of sample 0"}),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": f"{args.steps} theta_1 lines of sample 0, {threads} threads"},
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if vmn_s is not None:
+        line["cpu_baseline"]["per_sample_vmn_s"] = vmn_s
     print(json.dumps(line))
-
-
 # ------------------------------------------------------------------------- GPU arm
-def _traffic_per_matrix(kernel):
-    """DRAM bytes per matrix of `kernel` from the committed ncu capture summary, if any."""
-    path = os.path.join(REPO, "profiles", "dram_traffic.json")
-    try:
-        with open(path) as f:
-            d = json.load(f)
-        if d.get("n") != N_PHI:
-            return None
-        return d["bytes_per_matrix"].get(kernel)
-    except (OSError, ValueError, KeyError):
-        return None
+def _traffic_per_matrix(kernel, n=N_PHI):
+    """DRAM bytes per matrix of `kernel` at order n from the committed ncu capture summaries
+    (profiles/dram_traffic*.json), if one covers that order."""
+    import glob
+    for path in sorted(glob.glob(os.path.join(REPO, "profiles", "dram_traffic*.json"))):
+        try:
+            with open(path) as f:
+                d = json.load(f)
+            if d.get("n") == n and kernel in d.get("bytes_per_matrix", {}):
+                return d["bytes_per_matrix"][kernel]
+        except (OSError, ValueError):
+            continue
+    return None
 
 
 # algorithmic FP64 flops per matrix of n_phi (LAPACK counts: zhetrd 16/3 n^3, zunmtr 8 n^3)
@@ -377,7 +470,6 @@ def run_gpu(args):
 RLM_WORKLOADS = {
     # name: (n_phi, g, samples per step) -- rlm with impurity concentration 16, +-1 strengths
     "rlm512": (512, 16, 32),
-    "rlm3000": (3000, 4, 8),
 }
 
 
@@ -443,6 +535,243 @@ def run_gpu_rlm(args):
     print(json.dumps(line), flush=True)
 
 
+def _measured_peaks():
+    """MEASURED_PEAKS.json (written by the pool's driver beside the repository), or {}."""
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _peak(peaks, key, fallback):
+    v = peaks.get(key)
+    if isinstance(v, (int, float)) and v > 0:
+        return float(v), "measured"
+    return fallback, "fallback"
+
+
+def _hlm_extra(ctx, steps=2):
+    """The hlm 48x16 configuration (n_phi=256, g=32, 64 samples per step), both modes, device
+    resident, a short run nested in the headline line."""
+    import numpy as np
+    import torch
+    import rlmb
+    pots = torch.tensor(rlmb.hlm_potentials(SEED, N_SITES, NS), device="cuda")
+    d_e = torch.empty((NS, N_PHI), dtype=torch.float64, device="cuda")
+    d_c = torch.empty((NS, N_PHI), dtype=torch.float64, device="cuda")
+    out = {"workload": _config()["workload"]}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {}
+    for mode in ("fp64", "mixed"):
+        ctx.precision = ctx.MIXED if mode == "mixed" else ctx.FP64
+        ctx.hlm_mesh_solve_device(LX, LY, Q, BAND, G, pots, d_e, d_c)
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(steps):
+            ctx.hlm_mesh_solve_device(LX, LY, Q, BAND, G, pots, d_e, d_c)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        res[mode] = (d_e.cpu().numpy(), d_c.cpu().numpy())
+        out[mode] = {"value": SOLVES_PER_STEP / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                     "samples_per_hour": NS / (ms * 1e-3) * 3600.0, "steps": steps, "warmup": 1}
+    ctx.precision = ctx.FP64
+    (e64, c64), (em, cm) = res["fp64"], res["mixed"]
+    out["chern_integral"] = bool(np.abs(c64 - np.rint(c64)).max() < 1e-6)
+    out["mixed"]["chern_integers_identical_to_fp64"] = bool(np.array_equal(np.rint(cm), np.rint(c64)))
+    out["mixed"]["max_energy_rel_error_vs_fp64"] = float(np.abs(em - e64).max() / np.abs(e64).max())
+    return out
+
+
+def run_headline(args):
+    """The headline: rlm n_phi=3000, g=4, 8 samples per step (see the module docstring)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import rlmb
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ctx = rlmb.Context(local)
+    n, g, ns = RLM_N, RLM_G, RLM_NS
+    seed = SEED + rank
+    solves = ns * RLM_KPTS
+    d_e = torch.empty((ns, n), dtype=torch.float64, device="cuda")
+    d_c = torch.empty((ns, n), dtype=torch.float64, device="cuda")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Sample indices stay small: the device draws sample s's disorder by skipping its MT19937
+    # stream ahead 3 * 48000 * s outputs, a cost that grows with s.
+    spare = [args.steps]   # next unused block of ns samples (blocks 0 .. steps-1 are the timed ones)
+
+    def fresh():
+        spare[0] += 1
+        return ns * (spare[0] - 1)
+
+    def timed(mode, steps, warmup, sampler=None):
+        """Warm-up steps on samples outside the timed range, then `steps` timed steps whose last
+        one solves samples 0 .. ns-1 (left in d_e, d_c).  Returns (max-over-ranks ms, profile,
+        launches, clocks)."""
+        ctx.precision = ctx.MIXED if mode == "mixed" else ctx.FP64
+        for w in range(warmup):
+            ctx.rlm_mesh_solve_device(n, 1.0, 16.0, g, seed, fresh(), d_e, d_c)
+        barrier()
+        if sampler:
+            sampler.start()
+        ctx.profile(True)
+        l0 = ctx.launches
+        barrier()
+        ev0.record()
+        for i in range(steps):
+            ctx.rlm_mesh_solve_device(n, 1.0, 16.0, g, seed, ns * (steps - 1 - i), d_e, d_c)
+        ev1.record()
+        barrier()
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        launches = ctx.launches - l0
+        prof = ctx.profile_report()
+        ctx.profile(False)
+        clk = sampler.stop() if sampler else None
+        return ms, prof, launches, clk
+
+    # ---- value: FP64 mode, device-resident results
+    ms_dev, prof, launches, clk = timed("fp64", args.steps, args.warmup, ClockSampler(torch.cuda.current_device()))
+    e64, c64 = d_e.cpu().numpy(), d_c.cpu().numpy()
+    # ---- e2e: the host-buffer C ABI (tables H2D, results D2H inside the timed region), FP64
+    e2e_steps = max(1, min(args.steps, 3))
+    ctx.precision = ctx.FP64
+    ctx.rlm_mesh_solve(n, 1.0, 16.0, g, seed, fresh(), ns)
+    e2e_samples = [fresh() for _ in range(e2e_steps)]
+    barrier()
+    ev0.record()
+    for s0 in e2e_samples:
+        ctx.rlm_mesh_solve(n, 1.0, 16.0, g, seed, s0, ns)
+    ev1.record()
+    barrier()
+    ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))
+    # ---- mixed mode on the same samples
+    m_steps = max(1, min(args.steps, 5))
+    ms_mix, prof_mix, _, _ = timed("mixed", m_steps, 3)
+    em, cm = d_e.cpu().numpy(), d_c.cpu().numpy()
+    ctx.precision = ctx.FP64
+    faults = ctx.tc_fault_count()
+    extra = _hlm_extra(ctx) if (ws == 1 and not args.no_extra) else None
+
+    value = ws * solves * args.steps / (ms_dev * 1e-3)
+    e2e = ws * solves * e2e_steps / (ms_e2e * 1e-3)
+    v_mix = ws * solves * m_steps / (ms_mix * 1e-3)
+    line = None
+    if rank == 0:
+        peaks = _measured_peaks()
+        fp64_peak = ctx.fp64_peak_tflops()
+        hbm, hbm_src = _peak(peaks, "hbm_gbs", 6650.0)
+        bf16, bf16_src = _peak(peaks, "bf16_tflops_sustained", 1400.0)
+        # parity of sample 0 against the reference's fixture (seed 1: rank 0)
+        par = None
+        if seed == 1 and os.path.exists(RLM_FIXTURE):
+            fx = np.load(RLM_FIXTURE)
+            eref, cref = fx["energies"][0], fx["chern"][0]
+            par = {"fixture": os.path.relpath(RLM_FIXTURE, REPO), "sample": 0}
+            for mode, (e, c) in (("fp64", (e64, c64)), ("mixed", (em, cm))):
+                par[mode] = {"max_energy_rel_error": float(np.abs(e[0] - eref).max() / np.abs(eref).max()),
+                             "chern_integers_identical": bool(np.array_equal(np.rint(c[0]), np.rint(cref))),
+                             "max_chern_deviation": float(np.abs(c[0] - cref).max())}
+        # dominant kernel label of the FP64 step and its FP64 roofline (algorithmic flops)
+        total_ms = sum(v[0] for v in prof.values())
+        kname, (kms, klaunch) = max(prof.items(), key=lambda kv: kv[1][0])
+        fpm = _kernel_flops_per_matrix(kname, n)
+        roof = None
+        if fpm is not None:
+            achieved = fpm * solves * args.steps / (kms * 1e-3) / 1e12
+            tr = _traffic_per_matrix(kname, n)
+            roof = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp64_peak, "traffic": tr * solves * args.steps / klaunch if tr else None,
+                    "peak_source": "measured in this run: FP64 FMA throughput probe (MEASURED_PEAKS.json holds "
+                                   "no FP64 figure)",
+                    "share_of_gpu_time": kms / total_ms, "launches": klaunch,
+                    "note": "achieved = 16/3 n^3 flops per matrix x matrices / the label's summed CUDA-event time; "
+                            "the k_hetrd label covers the panel kernels, their GEMM updates and the unblocked tail; "
+                            "traffic = ncu DRAM bytes per matrix (profiles/) x matrices per launch"}
+        eig_ms = sum(prof.get(k, (0, 0))[0] for k in ("k_hetrd", "k_stebz", "k_stein", "k_larft", "k_ormtr"))
+        eig_tf = 13.33 * n ** 3 * solves * args.steps / (eig_ms * 1e-3) / 1e12
+        # HBM-bound stages (a) assembly and (c) links / plaquettes: algorithmic bytes per step
+        hbm_bytes = {"k_rlm_assemble": 16.0 * n * n * solves,          # H written once
+                     "k_rlm_links": 16.0 * n * n * solves,             # each eigenvector matrix read once
+                     "k_plaquettes": (2 * 16.0 + 8.0) * n * solves}    # U1, U2 read, W read
+        roof_hbm = {}
+        for k, b in hbm_bytes.items():
+            if k in prof:
+                gbs = b * args.steps / (prof[k][0] * 1e-3) / 1e9
+                roof_hbm[k] = {"achieved_gbs": gbs, "peak_gbs": hbm, "frac": gbs / hbm, "peak_source": hbm_src}
+        # tensor-core products of the mixed mode (tcgen05, split TF32: 3 products per term)
+        tc = {}
+        tf32_peak = bf16 / 2.0
+        for k in ("k_ref_coupling", "k_ref_update"):
+            if k in prof_mix:
+                flops = 8.0 * n ** 3 * solves * m_steps * 2   # two refinement steps, one N^3 complex GEMM each
+                tf = 3.0 * flops / (prof_mix[k][0] * 1e-3) / 1e12
+                tc[k] = {"achieved_tf32_tflops": tf, "useful_complex_tflops": tf / 3.0, "peak_tf32_tflops": tf32_peak,
+                         "frac": tf / tf32_peak,
+                         "peak_source": f"{bf16_src} bf16 dense / 2 (TF32 runs at half the BF16 rate)"}
+        mixed = {"value": v_mix, "unit": UNIT, "ms_per_step": ms_mix / m_steps, "steps": m_steps, "warmup": 3,
+                 "samples_per_hour": v_mix / RLM_KPTS * 3600.0,
+                 "samples_per_hour_ratio_to_fp64": v_mix / value,
+                 "refinement_steps": 2,
+                 "chern_integers_identical_to_fp64": bool(np.array_equal(np.rint(cm), np.rint(c64))),
+                 "max_chern_deviation_from_fp64": float(np.abs(cm - c64).max()),
+                 "max_energy_rel_error_vs_fp64": float(np.abs(em - e64).max() / np.abs(e64).max()),
+                 "tensor_core_roofline": tc, "tc_faults": faults,
+                 "kernel_ms_per_step": {k: v[0] / m_steps for k, v in sorted(prof_mix.items())}}
+        nb = 2 * 221 * 221 + 2 * (g + 1) * 221 + 2 * n * 221   # coefficient tables (complex) ...
+        h2d = 8 * nb + 2 * RLM_KPTS * ns * 4                    # ... + the theta lists
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _rlm_config({"parallelism": f"replicas x{ws} (sample-sharded)",
+                                   "api": "rlmb_rlm_mesh_solve_device (value), rlmb_rlm_mesh_solve (e2e)",
+                                   "samples_per_hour": value / RLM_KPTS * 3600.0,
+                                   "chern_integral": bool(np.abs(c64 - np.rint(c64)).max() < 1e-6),
+                                   "eigensolve_failures": int(ctx.last_failures)}),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(2 * ns * n * 8),
+                    "steps": e2e_steps},
+            "mixed": mixed,
+            "parity": par,
+            "roofline": roof,
+            "eigensolve_roofline": {"flops_per_solve": "13.33 n^3", "kernels": "hetrd+stebz+stein+larft+ormtr",
+                                    "achieved_tflops": eig_tf, "peak_tflops": fp64_peak, "frac": eig_tf / fp64_peak},
+            "roofline_hbm": roof_hbm,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "extra": {"hlm48x16": extra} if extra else None,
+        }
+    if ws > 1:
+        dist.barrier()
+    ctx.close()
+    if rank == 0:
+        line["cpu_baseline"] = cpu_baseline_rlm() if ws == 1 else None
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
 FSS_SIZES = (64, 128, 192, 256, 384, 512)
 
 
@@ -493,14 +822,43 @@ def run_gpu_fss(args):
 
 
 def run_probe(args):
-    """One rlmb_heevd_batched call on `batch` random Hermitian matrices of order n (the small
-    case the ncu captures under profiles/ are taken on)."""
+    """Small cases for profiler captures: --probe heevd runs one rlmb_heevd_batched call on
+    `batch` random Hermitian matrices of order n (--mixed: in the mixed mode); --probe tcgemm
+    runs three batched n x n x n complex GEMMs on the tcgen05 engine and one on the DMMA
+    engine, and prints their CUDA-event times; --probe rlm runs one rlm mesh solve of
+    `batch` samples at order n, g=4."""
     import numpy as np
     import torch
     import rlmb
     ctx = rlmb.Context(0)
     rng = np.random.default_rng(0)
     n, b = args.n, args.batch
+    if args.probe == "tcgemm":
+        at = torch.randn((b, n, n), dtype=torch.complex128, device="cuda")
+        bt = torch.randn((b, n, n), dtype=torch.complex128, device="cuda")
+        out = {}
+        for name, eng, reps in (("tf32x3", ctx.GEMM_TF32X3, 3), ("fp64_dmma", ctx.GEMM_FP64, 1)):
+            ctx.zgemm(at, bt, eng)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                ctx.zgemm(at, bt, eng)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            out[name] = {"ms": ms, "complex_tflops": 8.0 * n ** 3 * b / (ms * 1e-3) / 1e12}
+        print(json.dumps({"probe": "tcgemm", "n": n, "batch": b, "faults": ctx.tc_fault_count(), **out}))
+        return
+    if args.probe == "rlm":
+        if args.mixed:
+            ctx.precision = ctx.MIXED
+        ctx.rlm_mesh_solve(n, 1.0, 16.0, 4, SEED, 0, b)
+        torch.cuda.synchronize()
+        print(json.dumps({"probe": "rlm", "n": n, "samples": b, "launches": ctx.launches}))
+        return
+    if args.mixed:
+        ctx.precision = ctx.MIXED
     a0 = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
     a = torch.tensor(np.ascontiguousarray(a0 + np.conj(np.transpose(a0, (0, 2, 1)))), device="cuda")
     ctx.heevd(a)
@@ -511,15 +869,17 @@ def run_probe(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="hlm48x16", choices=["hlm48x16", "fss"] + sorted(RLM_WORKLOADS),
-                    help="hlm48x16 (default, the headline), an rlm configuration (1 GPU, both precisions), "
+    ap.add_argument("--workload", default="rlm3000", choices=["rlm3000", "hlm48x16", "rlm512", "fss"],
+                    help="rlm3000 (default, the headline), hlm48x16, rlm512 (1 GPU, both precisions), "
                          "or fss (the rlm finite-size-scaling sizes, 1 GPU)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the nested hlm48x16 block of the headline")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision measurement on the same inputs")
-    ap.add_argument("--probe", default=None, choices=["heevd"],
+    ap.add_argument("--mixed", action="store_true", help="probe in the mixed-precision mode")
+    ap.add_argument("--probe", default=None, choices=["heevd", "tcgemm", "rlm"],
                     help="run one small eigensolver batch only (for profiler captures)")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=296)
@@ -528,6 +888,8 @@ def main():
         run_probe(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.workload == "rlm3000":
+        run_headline(args)
     elif args.workload in RLM_WORKLOADS:
         run_gpu_rlm(args)
     elif args.workload == "fss":

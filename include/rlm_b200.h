@@ -86,16 +86,35 @@ int rlmb_heevd_host(rlmb_context* ctx, double* h_a, double* h_w, int n, int batc
  * It is for callers that cannot allocate device memory: processes whose device memory is
  * already reserved in full by another allocator (a framework's caching pool, a job's fixed
  * memory budget) and callers that must not take cudaMalloc/cudaFree's implicit device
- * synchronisation mid-run.  Same layout, arguments and results as rlmb_heevd_batched; no
- * context, work is queued on `stream` (a cudaStream_t, 0 = legacy default stream).
+ * synchronisation mid-run.  Same layout and arguments as rlmb_heevd_batched; it always
+ * solves in double precision (the FP64 mode, no mixed-precision refinement), whatever
+ * precision mode contexts use elsewhere.  No context: work is queued on `stream` (a
+ * cudaStream_t of the current device, 0 = legacy default stream; a stream of another
+ * device returns RLMB_ERR_ARG).  A launch error the caller left pending returns
+ * RLMB_ERR_CUDA at entry and is left in place.
  * Scratch is a fixed file-scope device array of RLMB_NOALLOC_SCRATCH_BYTES that every GPU
  * loading the library holds until exit; a matrix order whose scratch does not fit
- * (n > 927) returns RLMB_ERR_TOO_LARGE, larger batches are processed in chunks.  The first
- * call on each device looks the array's device address up (cudaGetSymbolAddress), so make
- * that first call before any stream capture.  All calls share the array: calls whose GPU
- * work overlaps in time (other streams or host threads) race. */
+ * (n > 927) returns RLMB_ERR_TOO_LARGE, larger batches are processed in equal chunks.  The
+ * first call on each device looks the array's device address up (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  All calls share the array: calls whose
+ * GPU work overlaps in time (other streams or host threads) race. */
 #define RLMB_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int rlmb_heevd_batched_noalloc(double* d_a, double* d_w, int n, int batch, int* d_info, void* stream);
+
+/* Batched complex GEMM C = A B on the device (no counterpart in the reference, whose dense
+ * products are MKL cblas_zgemm3m calls, hlm/hamiltonian_hlm_cpu.cpp:176,180): d_a, d_b, d_c
+ * hold batch column-major complex matrices back to back (A m x k, B k x n, C m x n).
+ * engine RLMB_GEMM_FP64: double precision on the FP64 tensor path (DMMA);
+ * engine RLMB_GEMM_TF32X3: the tcgen05 tensor cores, each operand split into two TF32
+ * numbers and three products accumulated in FP32 (relative error ~1e-6 of |A||B|), the
+ * engine of the mixed-precision eigensolver's products.  batch <= 65535. */
+#define RLMB_GEMM_FP64 0
+#define RLMB_GEMM_TF32X3 1
+int rlmb_zgemm_batched(rlmb_context* ctx, const double* d_a, const double* d_b, double* d_c, int m, int n,
+                       int k, int batch, int engine);
+/* Tiles of the tcgen05 engine whose bounded mbarrier waits ran out (a fault: the tile's
+ * output is not written) since the library was loaded; synchronises the device. */
+int rlmb_tc_fault_count(rlmb_context* ctx, int* count);
 
 /* ------------------------------------------------------- (a) rlm assembly
  * Disorder-independent coefficient tables, computed on the host exactly as
@@ -127,7 +146,7 @@ int rlmb_rlm_assemble(rlmb_context* ctx, const double* d_vmn, const double* d_co
 
 /* ------------------------------------------------------- (a) hlm assembly
  * On-site potentials of n_sample samples from one run-long stream
- * (hlm/main_hlm_cpu.cpp:345-358): h_out[n_sample*n_sites]. */
+ * (hlm/main_hlm_cpu.cpp:66-67,79): h_out[n_sample*n_sites]. */
 int rlmb_hlm_potentials(unsigned long seed, int n_sites, int n_sample, double* h_out);
 /* hlm potentials of samples sample0 .. sample0+count-1 drawn on the device (outputs
  * [sample*n_sites, (sample+1)*n_sites) of the run's single stream), bit-identical to
@@ -159,6 +178,12 @@ int rlmb_fhs_line(rlmb_context* ctx, const double* d_prev, const double* d_cur, 
 int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double quanta_concentration,
                         double impurity_concentration, int n_mesh, unsigned long seed,
                         int sample0, int n_samples, double* h_energies, double* h_chern);
+/* Device-resident form: energies and Chern numbers go to device memory (d_energies, d_chern:
+ * n_samples*n_phi doubles each); the disorder is drawn on the device as in
+ * rlmb_rlm_mesh_solve, so nothing but the call's parameters crosses from the host. */
+int rlmb_rlm_mesh_solve_device(rlmb_context* ctx, int n_phi, double quanta_concentration,
+                               double impurity_concentration, int n_mesh, unsigned long seed,
+                               int sample0, int n_samples, double* d_energies, double* d_chern);
 /* rlm, one sample, with its eigenvectors exported: besides the energies and Chern numbers
  * of rlmb_rlm_mesh_solve, every k-point's eigenvector matrix is written to
  * dir/wfs_<theta_1>_<theta_2>.bin (theta_1, theta_2 in 0..n_mesh) in the raw format of the
@@ -169,7 +194,25 @@ int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double quanta_concentratio
 int rlmb_rlm_mesh_export(rlmb_context* ctx, int n_phi, double quanta_concentration,
                          double impurity_concentration, int n_mesh, unsigned long seed, int sample,
                          const char* dir, double* h_energies, double* h_chern);
-/* hlm: n_samples samples with the given potentials (hlm/main_hlm_cpu.cpp:354-475). */
+/* Several rlm orders in ONE CUDA graph launch per step (the finite-size-scaling batch; no
+ * counterpart in the reference, whose driver runs one n_phi per process).  create prepares
+ * the pipeline of each order n_phi[0..count) (its own stream and buffers, every buffer sized
+ * by one uncaptured run of samples 0 .. n_samples-1) and captures all of them, one concurrent
+ * branch per order, in precision mode `precision` (RLMB_PRECISION_FP64 or _MIXED).  launch
+ * queues one step -- samples sample0 .. sample0+n_samples-1 of every order -- on the graph's
+ * stream (stream returns it, a cudaStream_t) without synchronising; results synchronises and
+ * copies order `index`'s energies and Chern numbers of the last step (n_samples*n_phi each,
+ * the columns of energy_Chern_No.txt) and returns its failure count. */
+typedef struct rlmb_fss_graph rlmb_fss_graph;
+int rlmb_rlm_fss_graph_create(int device, const int* n_phi, int count, double quanta_concentration,
+                              double impurity_concentration, int n_mesh, unsigned long seed, int n_samples,
+                              int precision, rlmb_fss_graph** graph);
+int rlmb_rlm_fss_graph_launch(rlmb_fss_graph* graph, int sample0);
+int rlmb_rlm_fss_graph_stream(rlmb_fss_graph* graph, void** stream);
+int rlmb_rlm_fss_graph_results(rlmb_fss_graph* graph, int index, double* h_energies, double* h_chern);
+int rlmb_rlm_fss_graph_destroy(rlmb_fss_graph* graph);
+
+/* hlm: n_samples samples with the given potentials (hlm/main_hlm_cpu.cpp:75-197). */
 int rlmb_hlm_mesh_solve(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh,
                         const double* h_potentials, int n_samples, double* h_energies,
                         double* h_chern);

@@ -67,6 +67,38 @@ void ref_rlm_solve_line(int theta_1, int n_phi, int n_mesh, int dim, int off_hea
     for (int id = 0; id < num_threads; ++id) pthread_join(th[id], NULL);
 }
 
+// The k-points (theta_1, theta_2[i]), i < count, of one line: assembly + heevd by the
+// reference's peer_solve_projected, the list dealt round-robin over num_threads threads (a
+// bounded sample of a line for the CPU baseline of large orders).
+void ref_rlm_solve_list(int theta_1, const int* theta_2, int count, int n_phi, int n_mesh, int dim, int off_head,
+                        std::complex<double>* wave_functions, double* energy_theta, std::complex<double>* v_mn,
+                        std::complex<double>* coeff_jm, std::complex<double>* coeff_m_theta, int num_threads) {
+    std::vector<std::vector<int>> lists(num_threads);
+    for (int i = 0; i < count; ++i) lists[i % num_threads].push_back(theta_2[i]);
+    std::vector<struct_solve> params(num_threads);
+    std::vector<pthread_t> th(num_threads);
+    int started = 0;
+    for (int id = 0; id < num_threads; ++id) {
+        if (lists[id].empty()) break;
+        params[id].theta_1 = theta_1;
+        params[id].n_phi = n_phi;
+        params[id].n_mesh = n_mesh;
+        params[id].dim_m = dim;
+        params[id].dim_n = dim;
+        params[id].off_head = off_head;
+        params[id].theta_2 = lists[id].data();
+        params[id].theta_len = (int)lists[id].size();
+        params[id].wave_function = wave_functions;
+        params[id].energy = energy_theta;
+        params[id].v_mn = v_mn;
+        params[id].coeff_jm = coeff_jm;
+        params[id].coeff_m_theta = coeff_m_theta;
+        pthread_create(&th[id], NULL, peer_solve_projected, (void*)&params[id]);
+        ++started;
+    }
+    for (int id = 0; id < started; ++id) pthread_join(th[id], NULL);
+}
+
 // FHS Chern contributions of the plaquettes between lines theta_1-1 and theta_1,
 // diag_wrappers/chern.cpp:37-75 dealt over threads as rlm/main_rlm_cpu.cpp:195-208.
 // chern_theta is n_mesh*n_phi, entry [m + n*n_mesh].

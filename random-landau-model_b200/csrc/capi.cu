@@ -14,6 +14,7 @@ void prof_free(rlmb_context* ctx);
 
 static int grow(rlmb_context* ctx, void** buf, size_t* have, size_t bytes) {
     if (bytes <= *have) return RLMB_OK;
+    if (ctx->frozen) return RLMB_ERR_ALLOC;   // a stream capture is recording: no reallocation
     if (*buf) {
         RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         RLMB_CUDA_TRY(cudaFree(*buf));
@@ -31,6 +32,7 @@ static int grow(rlmb_context* ctx, void** buf, size_t* have, size_t bytes) {
 }
 int ensure_workspace(rlmb_context* ctx, size_t bytes) { return grow(ctx, &ctx->ws, &ctx->ws_bytes, bytes); }
 int ensure_pipe(rlmb_context* ctx, size_t bytes) { return grow(ctx, &ctx->pipe, &ctx->pipe_bytes, bytes); }
+static int ensure_io(rlmb_context* ctx, size_t bytes) { return grow(ctx, &ctx->io, &ctx->io_bytes, bytes); }
 int ensure_pinned(rlmb_context* ctx, size_t bytes) {
     if (bytes <= ctx->pinned_bytes) return RLMB_OK;
     if (ctx->pinned) {
@@ -96,13 +98,37 @@ static int hlm_tables(rlmb_context* ctx, int lx, int ly, int Q, int band, int g,
     return RLMB_OK;
 }
 
-// Adds the number of nonzero entries of d_info[0..count) to *failures (synchronous).
-static int count_failures(rlmb_context* ctx, const int* d_info, int count, long long* failures) {
-    std::vector<int> h(count);
-    RLMB_CUDA_TRY(cudaMemcpyAsync(h.data(), d_info, count * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    for (int i = 0; i < count; ++i) *failures += h[i] != 0;
+// Eigensolve failures of a pipeline call are tallied on the device (no host round trip per
+// batch) and read once, when the call ends.
+__global__ void k_count_nonzero(const int* __restrict__ info, int count, int* __restrict__ fail) {
+    int c = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) c += info[i] != 0;
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(fail, c);
+}
+static int reset_failures(rlmb_context* ctx) {
+    if (!ctx->fail) {
+        if (cudaMalloc(reinterpret_cast<void**>(&ctx->fail), sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->fail = nullptr;
+            return RLMB_ERR_ALLOC;
+        }
+    }
+    RLMB_CUDA_TRY(cudaMemsetAsync(ctx->fail, 0, sizeof(int), ctx->stream));
     return RLMB_OK;
+}
+static int tally_failures(rlmb_context* ctx, const int* d_info, int count) {
+    if (count <= 0) return RLMB_OK;
+    k_count_nonzero<<<std::min((count + 255) / 256, 1024), 256, 0, ctx->stream>>>(d_info, count, ctx->fail);
+    RLMB_LAUNCHED(ctx);
+    return RLMB_OK;
+}
+// Synchronises the context stream and returns the call's status: the failure count, if any.
+static int finish_call(rlmb_context* ctx) {
+    int h = 0;
+    RLMB_CUDA_TRY(cudaMemcpyAsync(&h, ctx->fail, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return h > 0 ? h : RLMB_OK;
 }
 
 static bool hlm_args_ok(int lx, int ly, int Q, int band, int g) {
@@ -164,6 +190,9 @@ int rlmb_destroy(rlmb_context* ctx) {
     prof_free(ctx);
     if (ctx->ws) cudaFree(ctx->ws);
     if (ctx->pipe) cudaFree(ctx->pipe);
+    if (ctx->io) cudaFree(ctx->io);
+    if (ctx->fail) cudaFree(ctx->fail);
+    if (ctx->mt_state) cudaFree(ctx->mt_state);
     if (ctx->hlm_tables) cudaFree(ctx->hlm_tables);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     delete ctx;
@@ -373,29 +402,42 @@ static int export_wfs(rlmb_context* ctx, const cplx* d_H, int n, int g, const ch
 }
 
 static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh, unsigned long seed,
-                    int sample0, int n_samples, double* h_energies, double* h_chern, const char* wfs_dir);
+                    int sample0, int n_samples, double* energies, double* chern, bool dev_out, const char* wfs_dir);
 
 int rlmb_rlm_mesh_solve(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh,
                         unsigned long seed, int sample0, int n_samples, double* h_energies,
                         double* h_chern) {
-    return rlm_mesh(ctx, n_phi, qc, ic, n_mesh, seed, sample0, n_samples, h_energies, h_chern, nullptr);
+    return rlm_mesh(ctx, n_phi, qc, ic, n_mesh, seed, sample0, n_samples, h_energies, h_chern, false, nullptr);
+}
+
+int rlmb_rlm_mesh_solve_device(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh,
+                               unsigned long seed, int sample0, int n_samples, double* d_energies,
+                               double* d_chern) {
+    return rlm_mesh(ctx, n_phi, qc, ic, n_mesh, seed, sample0, n_samples, d_energies, d_chern, true, nullptr);
 }
 
 int rlmb_rlm_mesh_export(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh,
                          unsigned long seed, int sample, const char* dir, double* h_energies,
                          double* h_chern) {
     if (!dir) return RLMB_ERR_ARG;
-    return rlm_mesh(ctx, n_phi, qc, ic, n_mesh, seed, sample, 1, h_energies, h_chern, dir);
+    return rlm_mesh(ctx, n_phi, qc, ic, n_mesh, seed, sample, 1, h_energies, h_chern, false, dir);
 }
 
-static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh, unsigned long seed,
-                    int sample0, int n_samples, double* h_energies, double* h_chern, const char* wfs_dir) {
-    if (!ctx || n_phi <= 0 || !(qc > 0) || !(ic > 0) || n_mesh <= 0 || sample0 < 0 || n_samples < 0 ||
-        (n_samples > 0 && (!h_energies || !h_chern)))
-        return RLMB_ERR_ARG;
-    if (n_samples == 0) return RLMB_OK;
-    RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
-    // derived sizes, with the reference's C truncations (rlm/main_rlm_cpu.cpp:29-33)
+// One prepared rlm pipeline geometry: sizes, the batch of samples, and the regions of the
+// context's pipeline buffer (coefficient tables and theta lists uploaded once).
+struct RlmPlan {
+    int n_phi, nimp, o, dim, g, kpts, nb, n_samples;
+    double L1, L2;
+    unsigned long seed;
+    cplx *d_cmn, *d_cmt, *d_cjm, *d_vmn, *d_H, *d_U;
+    double *d_imp, *d_W, *d_out;
+    int *d_t, *d_info;
+};
+
+// Sizes (with the reference's C truncations, rlm/main_rlm_cpu.cpp:29-33), buffers and the
+// disorder-independent tables of an rlm mesh call; synchronises the context stream.
+static int rlm_prepare(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh, unsigned long seed,
+                       int n_samples, RlmPlan* p) {
     const double L1 = std::sqrt(n_phi * qc), L2 = std::sqrt(n_phi * qc);
     const long nimp_l = (long)(ic * n_phi / qc);
     const long o_l = (long)(std::sqrt((double)nimp_l) / 2 + 1);
@@ -403,13 +445,12 @@ static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_me
     const int nimp = (int)nimp_l, o = (int)o_l, dim = 2 * o + 1;
     const int g = n_mesh, kpts = (g + 1) * (g + 1);
     const size_t nn = (size_t)n_phi * n_phi;
-    // host tables
     std::vector<double> cmn(2 * (size_t)dim * dim), cmt(2 * (size_t)(g + 1) * dim), cjm(2 * (size_t)n_phi * dim);
     if (int rc = rlmb_rlm_coeff_tables(n_phi, o, dim, g, L1, L2, cmn.data(), cmt.data(), cjm.data())) return rc;
     // batch of samples that fits the budget
     const size_t per_sample = kpts * (nn * sizeof(cplx) + (size_t)n_phi * (sizeof(double) + 2 * sizeof(cplx))) +
                               (size_t)dim * dim * sizeof(cplx) + 3 * (size_t)nimp * sizeof(double);
-    int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx) / per_sample);
+    const int nb = balanced_batch(n_samples, mesh_budget_bytes(ctx) / per_sample);
     size_t bytes = 0;
     need<cplx>(bytes, cmn.size() / 2);
     need<cplx>(bytes, cmt.size() / 2);
@@ -424,63 +465,281 @@ static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_me
     need<int>(bytes, (size_t)kpts * nb);
     if (int rc = ensure_pipe(ctx, bytes)) return rc;
     Carver cv(ctx->pipe);
-    cplx* d_cmn = cv.take<cplx>(cmn.size() / 2);
-    cplx* d_cmt = cv.take<cplx>(cmt.size() / 2);
-    cplx* d_cjm = cv.take<cplx>(cjm.size() / 2);
-    double* d_imp = cv.take<double>(3 * (size_t)nimp * nb);
-    cplx* d_vmn = cv.take<cplx>((size_t)dim * dim * nb);
-    int* d_t = cv.take<int>(2 * (size_t)kpts * nb);
-    cplx* d_H = cv.take<cplx>(nn * kpts * nb);
-    double* d_W = cv.take<double>((size_t)n_phi * kpts * nb);
-    cplx* d_U = cv.take<cplx>(2 * (size_t)n_phi * kpts * nb);
-    double* d_out = cv.take<double>(2 * (size_t)n_phi * nb);
-    int* d_info = cv.take<int>((size_t)kpts * nb);
-    long long failures = 0;
-    if (int rc = ensure_pinned(ctx, std::max(3 * (size_t)nimp * nb * sizeof(double), 2 * (size_t)kpts * nb * sizeof(int))))
-        return rc;
-    RLMB_CUDA_TRY(cudaMemcpyAsync(d_cmn, cmn.data(), cmn.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    RLMB_CUDA_TRY(cudaMemcpyAsync(d_cmt, cmt.data(), cmt.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    RLMB_CUDA_TRY(cudaMemcpyAsync(d_cjm, cjm.data(), cjm.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    {
-        int* pt = static_cast<int*>(ctx->pinned);
-        for (int s = 0; s < nb; ++s)
-            for (int t = 0; t < kpts; ++t) {
-                pt[s * kpts + t] = t / (g + 1);
-                pt[(size_t)nb * kpts + s * kpts + t] = t % (g + 1);
-            }
-        RLMB_CUDA_TRY(cudaMemcpyAsync(d_t, pt, 2 * (size_t)kpts * nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    }
-    for (int s0 = 0; s0 < n_samples; s0 += nb) {
-        const int cnt = std::min(nb, n_samples - s0);
+    *p = RlmPlan{};
+    p->n_phi = n_phi;
+    p->nimp = nimp;
+    p->o = o;
+    p->dim = dim;
+    p->g = g;
+    p->kpts = kpts;
+    p->nb = nb;
+    p->n_samples = n_samples;
+    p->L1 = L1;
+    p->L2 = L2;
+    p->seed = seed;
+    p->d_cmn = cv.take<cplx>(cmn.size() / 2);
+    p->d_cmt = cv.take<cplx>(cmt.size() / 2);
+    p->d_cjm = cv.take<cplx>(cjm.size() / 2);
+    p->d_imp = cv.take<double>(3 * (size_t)nimp * nb);
+    p->d_vmn = cv.take<cplx>((size_t)dim * dim * nb);
+    p->d_t = cv.take<int>(2 * (size_t)kpts * nb);
+    p->d_H = cv.take<cplx>(nn * kpts * nb);
+    p->d_W = cv.take<double>((size_t)n_phi * kpts * nb);
+    p->d_U = cv.take<cplx>(2 * (size_t)n_phi * kpts * nb);
+    p->d_out = cv.take<double>(2 * (size_t)n_phi * nb);
+    p->d_info = cv.take<int>((size_t)kpts * nb);
+    if (int rc = ensure_pinned(ctx, 2 * (size_t)kpts * nb * sizeof(int))) return rc;
+    if (int rc = ensure_workspace(ctx, rlm_potential_ws_elems(nimp, nb, dim) * sizeof(cplx))) return rc;
+    RLMB_CUDA_TRY(cudaMemcpyAsync(p->d_cmn, cmn.data(), cmn.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    RLMB_CUDA_TRY(cudaMemcpyAsync(p->d_cmt, cmt.data(), cmt.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    RLMB_CUDA_TRY(cudaMemcpyAsync(p->d_cjm, cjm.data(), cjm.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    int* pt = static_cast<int*>(ctx->pinned);
+    for (int s = 0; s < nb; ++s)
+        for (int t = 0; t < kpts; ++t) {
+            pt[s * kpts + t] = t / (g + 1);
+            pt[(size_t)nb * kpts + s * kpts + t] = t % (g + 1);
+        }
+    RLMB_CUDA_TRY(cudaMemcpyAsync(p->d_t, pt, 2 * (size_t)kpts * nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    // the host tables are call-local and the pinned staging is reused by the next call: both
+    // copies must have completed before this function returns
+    RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return RLMB_OK;
+}
+
+// The stream-ordered work of an rlm mesh call on a prepared plan: samples sample0 ..
+// sample0 + n_samples - 1 (plus *d_sample0 when given: the first sample index is then read
+// from device memory, for a captured graph), energies / chern n_samples * n_phi values each,
+// in device memory if dev_out, else in host memory.  No host round trips: eigensolve
+// failures are tallied on the device.
+static int rlm_enqueue(rlmb_context* ctx, const RlmPlan& p, int sample0, const int* d_sample0, double* energies,
+                       double* chern, bool dev_out, const char* wfs_dir) {
+    const int n_phi = p.n_phi, nimp = p.nimp, nb = p.nb, kpts = p.kpts, g = p.g, dim = p.dim, o = p.o;
+    for (int s0 = 0; s0 < p.n_samples; s0 += nb) {
+        const int cnt = std::min(nb, p.n_samples - s0);
+        double* dx = p.d_imp;
+        double* dy = p.d_imp + (size_t)nb * nimp;
+        double* ds = p.d_imp + 2 * (size_t)nb * nimp;
         // disorder drawn on the device, bit-identical to the host stream (csrc/disorder.cu)
-        if (int rc = rlmb_rlm_disorder_device(ctx, nimp, L1, L2, seed, sample0 + s0, cnt, d_imp,
-                                              d_imp + (size_t)nb * nimp, d_imp + 2 * (size_t)nb * nimp))
+        if (d_sample0) {
+            if (int rc = launch_rlm_disorder_at(ctx, nimp, p.L1, p.L2, p.seed, d_sample0, sample0 + s0, cnt, dx, dy, ds))
+                return rc;
+        } else if (int rc = rlmb_rlm_disorder_device(ctx, nimp, p.L1, p.L2, p.seed, sample0 + s0, cnt, dx, dy, ds)) {
             return rc;
-        if (int rc = ensure_workspace(ctx, rlm_potential_ws_elems(nimp, cnt, dim) * sizeof(cplx))) return rc;
-        if (int rc = launch_rlm_potential(ctx, d_imp, d_imp + (size_t)nb * nimp, d_imp + 2 * (size_t)nb * nimp,
-                                          nimp, cnt, d_cmn, dim, o, static_cast<cplx*>(ctx->ws), d_vmn))
+        }
+        if (int rc = launch_rlm_potential(ctx, dx, dy, ds, nimp, cnt, p.d_cmn, dim, o, static_cast<cplx*>(ctx->ws),
+                                          p.d_vmn))
             return rc;
-        if (int rc = launch_rlm_assemble(ctx, d_vmn, d_cmt, d_cjm, d_t, d_t + (size_t)nb * kpts, cnt * kpts, kpts,
-                                         n_phi, dim, o, d_H))
+        if (int rc = launch_rlm_assemble(ctx, p.d_vmn, p.d_cmt, p.d_cjm, p.d_t, p.d_t + (size_t)nb * kpts, cnt * kpts,
+                                         kpts, n_phi, dim, o, p.d_H))
             return rc;
-        if (int rc = rlmb_heevd_batched(ctx, reinterpret_cast<double*>(d_H), d_W, n_phi, cnt * kpts, d_info))
+        if (int rc = heevd_batched_band(ctx, reinterpret_cast<double*>(p.d_H), p.d_W, n_phi, cnt * kpts, p.d_info, o))
             return rc;
-        if (int rc = count_failures(ctx, d_info, cnt * kpts, &failures)) return rc;
+        if (int rc = tally_failures(ctx, p.d_info, cnt * kpts)) return rc;
         if (wfs_dir)
-            if (int rc = export_wfs(ctx, d_H, n_phi, g, wfs_dir)) return rc;   // one sample (cnt == 1)
-        cplx* d_U1 = d_U;
-        cplx* d_U2 = d_U + (size_t)n_phi * kpts * nb;
-        if (int rc = launch_rlm_links(ctx, d_H, n_phi, g, cnt, d_U1, d_U2)) return rc;
-        if (int rc = launch_plaquettes(ctx, d_U1, d_U2, d_W, n_phi, g, cnt, 0, d_out, d_out + (size_t)n_phi * nb))
-            return rc;
-        RLMB_CUDA_TRY(cudaMemcpyAsync(h_energies + (size_t)s0 * n_phi, d_out, (size_t)cnt * n_phi * sizeof(double),
-                                      cudaMemcpyDeviceToHost, ctx->stream));
-        RLMB_CUDA_TRY(cudaMemcpyAsync(h_chern + (size_t)s0 * n_phi, d_out + (size_t)n_phi * nb,
-                                      (size_t)cnt * n_phi * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            if (int rc = export_wfs(ctx, p.d_H, n_phi, g, wfs_dir)) return rc;   // one sample (cnt == 1)
+        cplx* d_U1 = p.d_U;
+        cplx* d_U2 = p.d_U + (size_t)n_phi * kpts * nb;
+        if (int rc = launch_rlm_links(ctx, p.d_H, n_phi, g, cnt, d_U1, d_U2)) return rc;
+        double* out_e = dev_out ? energies + (size_t)s0 * n_phi : p.d_out;
+        double* out_c = dev_out ? chern + (size_t)s0 * n_phi : p.d_out + (size_t)n_phi * nb;
+        if (int rc = launch_plaquettes(ctx, d_U1, d_U2, p.d_W, n_phi, g, cnt, 0, out_e, out_c)) return rc;
+        if (!dev_out) {
+            RLMB_CUDA_TRY(cudaMemcpyAsync(energies + (size_t)s0 * n_phi, p.d_out, (size_t)cnt * n_phi * sizeof(double),
+                                          cudaMemcpyDeviceToHost, ctx->stream));
+            RLMB_CUDA_TRY(cudaMemcpyAsync(chern + (size_t)s0 * n_phi, p.d_out + (size_t)n_phi * nb,
+                                          (size_t)cnt * n_phi * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        }
     }
-    return failures > 0 ? (int)std::min<long long>(failures, 1 << 30) : RLMB_OK;
+    return RLMB_OK;
+}
+
+// The rlm pipeline: energies / chern receive n_samples * n_phi values each, in device memory
+// if dev_out, else in host memory.  After its set-up the call's device work is stream-ordered
+// without host round trips between batches; it synchronises once, at the end, to return its
+// status.
+static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_mesh, unsigned long seed,
+                    int sample0, int n_samples, double* energies, double* chern, bool dev_out, const char* wfs_dir) {
+    if (!ctx || n_phi <= 0 || !(qc > 0) || !(ic > 0) || n_mesh <= 0 || sample0 < 0 || n_samples < 0 ||
+        (n_samples > 0 && (!energies || !chern)))
+        return RLMB_ERR_ARG;
+    if (n_samples == 0) return RLMB_OK;
+    RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
+    RlmPlan p;
+    if (int rc = rlm_prepare(ctx, n_phi, qc, ic, n_mesh, seed, n_samples, &p)) return rc;
+    if (int rc = reset_failures(ctx)) return rc;
+    if (int rc = rlm_enqueue(ctx, p, sample0, nullptr, energies, chern, dev_out, wfs_dir)) return rc;
+    return finish_call(ctx);
+}
+
+// ----------------------------------------------- rlm orders captured in one CUDA graph
+// Several rlm mesh geometries (a finite-size-scaling set of n_phi) solved by ONE graph launch
+// per step.  Each order has its own library context (stream, workspace, pipeline buffers and
+// failure counter), prepared and run once outside the capture so that every buffer has its
+// final size; the capture then forks one branch per order from the graph's origin stream,
+// records each order's whole pipeline (disorder, V_mn, assembly, eigensolve, links,
+// plaquettes, device-side failure tally) on its context stream, and joins them.  The orders
+// run concurrently on the device: the small ones fill the SMs the large ones leave idle.
+// The first sample of a launch is written to device memory just before the graph runs, and
+// the disorder kernels read it there.
+struct FssOrder {
+    rlmb_context* ctx;
+    RlmPlan plan;
+    double* d_e;   // n_samples * n_phi energies, then as many Chern numbers
+    cudaEvent_t done;
+};
+
+struct rlmb_fss_graph {
+    int device;
+    int n_samples;
+    std::vector<FssOrder> orders;
+    cudaStream_t origin;
+    cudaEvent_t fork;
+    int* d_sample0;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+};
+
+__global__ void k_store_int(int* p, int v) { *p = v; }
+
+static void fss_release(rlmb_fss_graph* f) {
+    if (!f) return;
+    cudaSetDevice(f->device);
+    if (f->origin) cudaStreamSynchronize(f->origin);
+    if (f->exec) cudaGraphExecDestroy(f->exec);
+    if (f->graph) cudaGraphDestroy(f->graph);
+    for (FssOrder& o : f->orders) {
+        if (o.ctx) {
+            cudaStream_t st = o.ctx->stream;
+            rlmb_destroy(o.ctx);
+            if (st) cudaStreamDestroy(st);
+        }
+        if (o.d_e) cudaFree(o.d_e);
+        if (o.done) cudaEventDestroy(o.done);
+    }
+    if (f->d_sample0) cudaFree(f->d_sample0);
+    if (f->fork) cudaEventDestroy(f->fork);
+    if (f->origin) cudaStreamDestroy(f->origin);
+    delete f;
+}
+
+int rlmb_rlm_fss_graph_create(int device, const int* n_phi, int count, double qc, double ic, int n_mesh,
+                              unsigned long seed, int n_samples, int precision, rlmb_fss_graph** out) {
+    if (!out) return RLMB_ERR_ARG;
+    *out = nullptr;
+    if (!n_phi || count <= 0 || count > 64 || !(qc > 0) || !(ic > 0) || n_mesh <= 0 || n_samples <= 0 ||
+        (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED))
+        return RLMB_ERR_ARG;
+    for (int i = 0; i < count; ++i)
+        if (n_phi[i] <= 0) return RLMB_ERR_ARG;
+    rlmb_fss_graph* f = new rlmb_fss_graph();
+    f->device = device;
+    f->n_samples = n_samples;
+    f->orders.resize(count);
+    for (FssOrder& o : f->orders) o = FssOrder{nullptr, RlmPlan{}, nullptr, nullptr};
+    f->origin = nullptr;
+    f->fork = nullptr;
+    f->d_sample0 = nullptr;
+    f->graph = nullptr;
+    f->exec = nullptr;
+    int rc = rlmb_create(&f->orders[0].ctx, device);   // (also validates the device)
+    if (rc == RLMB_OK) {
+        rlmb_destroy(f->orders[0].ctx);
+        f->orders[0].ctx = nullptr;
+    }
+    auto fail = [&](int code) {
+        fss_release(f);
+        return code;
+    };
+    if (rc) return fail(rc);
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&f->origin, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(&f->d_sample0), sizeof(int)) != cudaSuccess ||
+        cudaMemset(f->d_sample0, 0, sizeof(int)) != cudaSuccess)
+        return fail(RLMB_ERR_CUDA);
+    // set-up and one uncaptured run per order: every buffer reaches its final size
+    for (int i = 0; i < count; ++i) {
+        FssOrder& o = f->orders[i];
+        cudaStream_t st = nullptr;
+        if ((rc = rlmb_create(&o.ctx, device))) return fail(rc);
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&o.done, cudaEventDisableTiming) != cudaSuccess) {
+            if (st) cudaStreamDestroy(st);
+            return fail(RLMB_ERR_CUDA);
+        }
+        o.ctx->stream = st;
+        o.ctx->precision = precision;
+        if (cudaMalloc(reinterpret_cast<void**>(&o.d_e), 2 * (size_t)n_samples * n_phi[i] * sizeof(double)) != cudaSuccess)
+            return fail(RLMB_ERR_ALLOC);
+        if ((rc = rlm_prepare(o.ctx, n_phi[i], qc, ic, n_mesh, seed, n_samples, &o.plan))) return fail(rc);
+        if ((rc = reset_failures(o.ctx))) return fail(rc);
+        if ((rc = rlm_enqueue(o.ctx, o.plan, 0, f->d_sample0, o.d_e, o.d_e + (size_t)n_samples * n_phi[i], true,
+                              nullptr)))
+            return fail(rc);
+        if ((rc = finish_call(o.ctx)) < 0) return fail(rc);
+    }
+    // capture: fork, one branch per order, join
+    if (cudaStreamBeginCapture(f->origin, cudaStreamCaptureModeRelaxed) != cudaSuccess) return fail(RLMB_ERR_CUDA);
+    rc = cudaEventRecord(f->fork, f->origin) == cudaSuccess ? RLMB_OK : RLMB_ERR_CUDA;
+    for (int i = 0; i < count && rc == RLMB_OK; ++i) {
+        FssOrder& o = f->orders[i];
+        if (cudaStreamWaitEvent(o.ctx->stream, f->fork, 0) != cudaSuccess) {
+            rc = RLMB_ERR_CUDA;
+            break;
+        }
+        o.ctx->frozen = 1;
+        if (cudaMemsetAsync(o.ctx->fail, 0, sizeof(int), o.ctx->stream) != cudaSuccess) rc = RLMB_ERR_CUDA;
+        if (rc == RLMB_OK)
+            rc = rlm_enqueue(o.ctx, o.plan, 0, f->d_sample0, o.d_e, o.d_e + (size_t)n_samples * n_phi[i], true, nullptr);
+        o.ctx->frozen = 0;
+        if (rc == RLMB_OK && (cudaEventRecord(o.done, o.ctx->stream) != cudaSuccess ||
+                              cudaStreamWaitEvent(f->origin, o.done, 0) != cudaSuccess))
+            rc = RLMB_ERR_CUDA;
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(f->origin, &graph);
+    f->graph = graph;
+    if (rc == RLMB_OK && ec != cudaSuccess) rc = RLMB_ERR_CUDA;
+    if (rc != RLMB_OK) {
+        cudaGetLastError();
+        return fail(rc);
+    }
+    if (cudaGraphInstantiate(&f->exec, f->graph, 0) != cudaSuccess) return fail(RLMB_ERR_CUDA);
+    *out = f;
+    return RLMB_OK;
+}
+
+int rlmb_rlm_fss_graph_launch(rlmb_fss_graph* f, int sample0) {
+    if (!f || sample0 < 0) return RLMB_ERR_ARG;
+    RLMB_CUDA_TRY(cudaSetDevice(f->device));
+    k_store_int<<<1, 1, 0, f->origin>>>(f->d_sample0, sample0);
+    RLMB_CUDA_TRY(cudaGetLastError());
+    RLMB_CUDA_TRY(cudaGraphLaunch(f->exec, f->origin));
+    return RLMB_OK;
+}
+
+int rlmb_rlm_fss_graph_stream(rlmb_fss_graph* f, void** stream) {
+    if (!f || !stream) return RLMB_ERR_ARG;
+    *stream = f->origin;
+    return RLMB_OK;
+}
+
+int rlmb_rlm_fss_graph_results(rlmb_fss_graph* f, int index, double* h_energies, double* h_chern) {
+    if (!f || index < 0 || index >= (int)f->orders.size() || !h_energies || !h_chern) return RLMB_ERR_ARG;
+    RLMB_CUDA_TRY(cudaSetDevice(f->device));
+    RLMB_CUDA_TRY(cudaStreamSynchronize(f->origin));
+    const FssOrder& o = f->orders[index];
+    const size_t cnt = (size_t)f->n_samples * o.plan.n_phi;
+    RLMB_CUDA_TRY(cudaMemcpy(h_energies, o.d_e, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    RLMB_CUDA_TRY(cudaMemcpy(h_chern, o.d_e + cnt, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    int fails = 0;
+    RLMB_CUDA_TRY(cudaMemcpy(&fails, o.ctx->fail, sizeof(int), cudaMemcpyDeviceToHost));
+    return fails > 0 ? fails : RLMB_OK;
+}
+
+int rlmb_rlm_fss_graph_destroy(rlmb_fss_graph* f) {
+    if (!f) return RLMB_ERR_ARG;
+    fss_release(f);
+    return RLMB_OK;
 }
 
 // --------------------------------------------------------------------- hlm pipeline
@@ -516,7 +775,7 @@ int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int ban
     cplx* d_U1 = cv.take<cplx>((size_t)N * kpts * nb);
     cplx* d_U2 = cv.take<cplx>((size_t)N * kpts * nb);
     int* d_info = cv.take<int>((size_t)kpts * nb);
-    long long failures = 0;
+    if (int rc = reset_failures(ctx)) return rc;
     {
         std::vector<int> tl(kpts);
         for (int t1 = 0; t1 <= g; ++t1)
@@ -530,13 +789,13 @@ int rlmb_hlm_mesh_solve_device(rlmb_context* ctx, int lx, int ly, int Q, int ban
         if (int rc = launch_hlm_project(ctx, hb, d_vt, d_t, lx, ly, Q, kpts, cnt, d_H)) return rc;
         if (int rc = rlmb_heevd_batched(ctx, reinterpret_cast<double*>(d_H), d_W, N, cnt * kpts, d_info))
             return rc;
-        if (int rc = count_failures(ctx, d_info, cnt * kpts, &failures)) return rc;
+        if (int rc = tally_failures(ctx, d_info, cnt * kpts)) return rc;
         if (int rc = launch_hlm_links(ctx, hb, d_H, lx, ly, Q, g, cnt, d_U1, d_U2)) return rc;
         if (int rc = launch_plaquettes(ctx, d_U1, d_U2, d_W, N, g, cnt, 1, d_energies + (size_t)s0 * N,
                                        d_chern + (size_t)s0 * N))
             return rc;
     }
-    return failures > 0 ? (int)std::min<long long>(failures, 1 << 30) : RLMB_OK;
+    return finish_call(ctx);
 }
 
 int rlmb_hlm_mesh_solve(rlmb_context* ctx, int lx, int ly, int Q, int band, int n_mesh,
@@ -547,26 +806,20 @@ int rlmb_hlm_mesh_solve(rlmb_context* ctx, int lx, int ly, int Q, int band, int 
     if (n_samples == 0) return RLMB_OK;
     RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
     const int N = lx * ly / Q, ns = lx * ly;
-    double* d_io = nullptr;
     const size_t io = ((size_t)ns + 2 * (size_t)N) * n_samples;
-    RLMB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d_io), io * sizeof(double), ctx->stream));
-    int rc = RLMB_OK;
-    double* d_pot = d_io;
-    double* d_e = d_io + (size_t)ns * n_samples;
+    if (int rc = ensure_io(ctx, io * sizeof(double))) return rc;   // grow-only staging, kept by the context
+    double* d_pot = static_cast<double*>(ctx->io);
+    double* d_e = d_pot + (size_t)ns * n_samples;
     double* d_c = d_e + (size_t)N * n_samples;
-    if (cudaMemcpyAsync(d_pot, h_potentials, (size_t)ns * n_samples * sizeof(double), cudaMemcpyHostToDevice,
-                        ctx->stream) != cudaSuccess)
-        rc = RLMB_ERR_CUDA;
-    if (rc == RLMB_OK) rc = rlmb_hlm_mesh_solve_device(ctx, lx, ly, Q, band, n_mesh, d_pot, n_samples, d_e, d_c);
-    if (rc == RLMB_OK) {
-        if (cudaMemcpyAsync(h_energies, d_e, (size_t)N * n_samples * sizeof(double), cudaMemcpyDeviceToHost,
-                            ctx->stream) != cudaSuccess ||
-            cudaMemcpyAsync(h_chern, d_c, (size_t)N * n_samples * sizeof(double), cudaMemcpyDeviceToHost,
-                            ctx->stream) != cudaSuccess)
-            rc = RLMB_ERR_CUDA;
-    }
-    cudaFreeAsync(d_io, ctx->stream);
-    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = RLMB_ERR_CUDA;
+    RLMB_CUDA_TRY(cudaMemcpyAsync(d_pot, h_potentials, (size_t)ns * n_samples * sizeof(double), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    const int rc = rlmb_hlm_mesh_solve_device(ctx, lx, ly, Q, band, n_mesh, d_pot, n_samples, d_e, d_c);
+    if (rc < 0) return rc;
+    RLMB_CUDA_TRY(cudaMemcpyAsync(h_energies, d_e, (size_t)N * n_samples * sizeof(double), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    RLMB_CUDA_TRY(cudaMemcpyAsync(h_chern, d_c, (size_t)N * n_samples * sizeof(double), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    RLMB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return rc;
 }
 

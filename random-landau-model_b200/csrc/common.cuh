@@ -117,6 +117,20 @@ struct rlmb_context {
     // pinned host staging
     void* pinned;
     size_t pinned_bytes;
+    // device staging of the host-buffer pipeline calls, and the device counter of
+    // eigensolves that did not converge (accumulated on the device, read once per call)
+    void* io;
+    size_t io_bytes;
+    int* fail;
+    // the device rlm disorder stream of the last call (state words + block index), for
+    // continuing it when the next call starts at the next sample
+    uint32_t* mt_state;
+    // set while a stream capture records this context's work: buffers may not grow then
+    int frozen;
+    int mt_valid;
+    unsigned long mt_seed;
+    int mt_nimp;
+    long long mt_next;
     // cached hlm tables (Bloch vectors and link overlaps of one mesh geometry)
     int hlm_key[6];
     void* hlm_tables;
@@ -143,6 +157,8 @@ namespace rlmb {
 // Per-kernel event timing: prof_begin records a start event on the context stream
 // before a launch, prof_end the stop event after it (no-ops unless profiling is on).
 void prof_begin(rlmb_context* ctx, const char* kernel);
+// rlmb_heevd_batched with a structure hint (band >= 0: cyclic band of that half-bandwidth).
+int heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch, int* d_info, int band);
 void prof_end(rlmb_context* ctx);
 }  // namespace rlmb
 

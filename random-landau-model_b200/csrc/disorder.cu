@@ -50,6 +50,16 @@ __device__ __forceinline__ void mt_seed(uint32_t* mt, uint32_t seed) {
     __syncthreads();
 }
 
+// state words and the index of the output block they hold, for a later continuation
+__device__ __forceinline__ void mt_save(const uint32_t* mt, long long blk, uint32_t* out) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < MT_N; i += blockDim.x) out[i] = mt[i];
+    if (threadIdx.x == 0) {
+        out[MT_N] = (uint32_t)((uint64_t)blk & 0xffffffffu);
+        out[MT_N + 1] = (uint32_t)((uint64_t)blk >> 32);
+    }
+}
+
 // a + (b - a) * u / 2^32 with the host's roundings (no contraction)
 __device__ __forceinline__ double mt_uniform(uint32_t u, double a, double b) {
     return __dadd_rn(a, __dmul_rn(b - a, __dmul_rn((double)u, 1.0 / 4294967296.0)));
@@ -60,9 +70,11 @@ __device__ __forceinline__ double mt_uniform(uint32_t u, double a, double b) {
 // output else -1.  Output [sample][i] in x, y, s (row stride ld).
 __global__ void __launch_bounds__(256)
 k_rlm_disorder(uint32_t seed, int nimp, double L1, double L2, int sample0, double* __restrict__ x,
-               double* __restrict__ y, double* __restrict__ s, size_t ld) {
+               double* __restrict__ y, double* __restrict__ s, size_t ld, uint32_t* __restrict__ save,
+               const int* __restrict__ dsample0) {
     __shared__ uint32_t mt[MT_N];
     const int smp = blockIdx.x;
+    if (dsample0) sample0 += *dsample0;   // first sample read from device memory (graph replays)
     mt_seed(mt, seed);
     long long pos = 3LL * nimp * (sample0 + smp);   // outputs consumed before this sample
     const long long end = pos + 3LL * nimp;
@@ -89,6 +101,49 @@ k_rlm_disorder(uint32_t seed, int nimp, double L1, double L2, int sample0, doubl
             ++blk;
         }
     }
+    if (save && smp == (int)gridDim.x - 1) mt_save(mt, blk, save);   // the stream after the last sample
+}
+
+// The same draws for samples sample0 .. sample0+count-1 by one CTA that continues the stream
+// from a state saved by an earlier call (the block of outputs holding position
+// 3 nimp sample0, and its index), generating the samples one after another: a run that
+// draws its samples in order pays each output once instead of a skip-ahead per sample.
+__global__ void __launch_bounds__(256)
+k_rlm_disorder_cont(int nimp, double L1, double L2, int sample0, int count, double* __restrict__ x,
+                    double* __restrict__ y, double* __restrict__ s, size_t ld, uint32_t* __restrict__ state) {
+    __shared__ uint32_t mt[MT_N];
+    __shared__ long long blk_s;
+    for (int i = threadIdx.x; i < MT_N; i += blockDim.x) mt[i] = state[i];
+    if (threadIdx.x == 0) blk_s = (long long)(((uint64_t)state[MT_N + 1] << 32) | state[MT_N]);
+    __syncthreads();
+    long long blk = blk_s;
+    const long long first = 3LL * nimp * sample0;
+    long long pos = first;
+    const long long end = first + 3LL * nimp * count;
+    while (blk < pos / MT_N) {   // (an earlier call may have stopped short of this block)
+        mt_twist(mt);
+        ++blk;
+    }
+    while (pos < end) {
+        const long long base = blk * MT_N;
+        for (long long k = pos + threadIdx.x; k < min(end, base + MT_N); k += blockDim.x) {
+            const uint32_t u = mt_temper(mt[k - base]);
+            const long long r = k - first;
+            const int smp = (int)(r / (3LL * nimp));
+            const long long q = r - 3LL * nimp * smp;
+            const int i = (int)(q % nimp), which = (int)(q / nimp);
+            if (which == 0) x[ld * smp + i] = mt_uniform(u, 0.0, L1);
+            else if (which == 1) y[ld * smp + i] = mt_uniform(u, 0.0, L2);
+            else s[ld * smp + i] = (u % 2u == 0u) ? 1.0 : -1.0;
+        }
+        pos = min(end, base + MT_N);
+        if (pos < end) {
+            __syncthreads();
+            mt_twist(mt);
+            ++blk;
+        }
+    }
+    mt_save(mt, blk, state);
 }
 
 // hlm on-site potentials (hlm/main_hlm_cpu.cpp:66-67,79): one stream for the whole run,
@@ -128,12 +183,50 @@ extern "C" int rlmb_rlm_disorder_device(rlmb_context* ctx, int impurity_num, dou
         return RLMB_ERR_ARG;
     if (count == 0) return RLMB_OK;
     RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
-    prof_begin(ctx, "k_rlm_disorder");
-    k_rlm_disorder<<<count, 256, 0, ctx->stream>>>((uint32_t)seed, impurity_num, L1, L2, sample0, d_x, d_y, d_s,
-                                                  (size_t)impurity_num);
+    if (!ctx->mt_state) {
+        if (cudaMalloc(reinterpret_cast<void**>(&ctx->mt_state), (MT_N + 2) * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->mt_state = nullptr;
+            return RLMB_ERR_ALLOC;
+        }
+        ctx->mt_valid = 0;
+    }
+    // continue the context's saved stream when this call starts where the last one ended
+    // (same seed and impurity count); otherwise every sample's CTA skips ahead on its own
+    const long long first = 3LL * impurity_num * sample0;
+    const bool cont = ctx->mt_valid && ctx->mt_seed == (unsigned long)(uint32_t)seed && ctx->mt_nimp == impurity_num &&
+                      ctx->mt_next == first;
+    if (cont) {
+        prof_begin(ctx, "k_rlm_disorder");
+        k_rlm_disorder_cont<<<1, 256, 0, ctx->stream>>>(impurity_num, L1, L2, sample0, count, d_x, d_y, d_s,
+                                                         (size_t)impurity_num, ctx->mt_state);
+    } else {
+        prof_begin(ctx, "k_rlm_disorder");
+        k_rlm_disorder<<<count, 256, 0, ctx->stream>>>((uint32_t)seed, impurity_num, L1, L2, sample0, d_x, d_y, d_s,
+                                                      (size_t)impurity_num, ctx->mt_state, nullptr);
+    }
     RLMB_LAUNCHED(ctx);
+    ctx->mt_valid = 1;
+    ctx->mt_seed = (unsigned long)(uint32_t)seed;
+    ctx->mt_nimp = impurity_num;
+    ctx->mt_next = first + 3LL * impurity_num * count;
     return RLMB_OK;
 }
+
+namespace rlmb {
+// rlm disorder of samples *d_sample0 + offset .. + count - 1, the first sample index read from
+// device memory when the kernel runs (for a captured graph replayed with new samples); no
+// stream state is saved or continued.
+int launch_rlm_disorder_at(rlmb_context* ctx, int nimp, double L1, double L2, unsigned long seed,
+                           const int* d_sample0, int offset, int count, double* d_x, double* d_y, double* d_s) {
+    prof_begin(ctx, "k_rlm_disorder");
+    k_rlm_disorder<<<count, 256, 0, ctx->stream>>>((uint32_t)seed, nimp, L1, L2, offset, d_x, d_y, d_s, (size_t)nimp,
+                                                  nullptr, d_sample0);
+    RLMB_LAUNCHED(ctx);
+    ctx->mt_valid = 0;
+    return RLMB_OK;
+}
+}  // namespace rlmb
 
 extern "C" int rlmb_hlm_potentials_device(rlmb_context* ctx, unsigned long seed, int n_sites, int sample0,
                                           int count, double* d_out) {

@@ -25,6 +25,7 @@
 #include "common.cuh"
 #include "small_eig.cuh"
 #include "zgemm.cuh"
+#include "zgemm_tc.cuh"
 
 #include <cfloat>
 #include <cmath>
@@ -1494,6 +1495,7 @@ struct EpHer2k {
     C* a;
     int n;
     __device__ __forceinline__ bool skip(int r0, int c0, int) const { return r0 > c0 + ZG_BN - 1; }
+    __device__ __forceinline__ bool skip_tile(int r0, int c0, int, int cols) const { return r0 > c0 + cols - 1; }
     __device__ __forceinline__ void store(size_t mat, int r, int c, C acc) const {
         if (r > c) return;
         C* q = a + mat * (size_t)n * n + (size_t)c * n + r;
@@ -1511,6 +1513,16 @@ struct EpHer2k {
         a[mat * (size_t)n * n + (size_t)c * n + r] = x;
     }
 };
+
+// The GEMMs of the reduction and back-transformation in the working precision C: double on
+// the FP64 tensor path (DMMA engine, BM-row tiles), single precision (the mixed mode) on the
+// tcgen05 tensor cores with split TF32 operands.
+template <class C, int BM, class LA, class LB, class EP>
+static cudaError_t launch_work_gemm(cudaStream_t st, const LA& la, const LB& lb, const EP& ep, int M, int N, int K,
+                                    int nb) {
+    if constexpr (std::is_same<C, cplxf>::value) return launch_zgemm_tc<C>(st, la, lb, ep, M, N, K, nb);
+    else return launch_zgemm<C, BM>(st, la, lb, ep, M, N, K, nb);
+}
 
 // ------------------------------------------------- mixed mode: FP64 refinement kernels
 // The mixed mode reduces and back-transforms in single precision (k_hetrd<.., float>,
@@ -1556,6 +1568,81 @@ struct EpResid {
         res[o] = mk(acc.x - lam * xr.x, acc.y - lam * xr.y);
     }
 };
+
+// R = H X - X diag(lambda) for a cyclic band matrix H of half-bandwidth o (H(r, k) = 0 unless
+// the cyclic distance of r and k is at most o -- the rlm Hamiltonian's structure,
+// rlm/hamiltonian_rlm_cpu.cpp:26-38), in double, with 32 + 2o <= n.  An output tile of 32 rows
+// x 64 columns needs only the 32 + 2o rows k = r0 - o .. r0 + 31 + o (cyclic) of X: the tile's
+// band rows of H, zero-padded to a dense 32 x (32 + 2o) block, times those rows of X, in
+// chunks of 16.  Row r of H is read as the conjugate of column r (contiguous in k) of the
+// Hermitian matrix stored in full.  Thread (tr, tc) computes rows 2 tr, 2 tr + 1 and columns
+// tc + 16 j (j < 4) of the tile: 8 complex multiply-adds per 6 shared-memory loads.
+template <class XT>
+__global__ void __launch_bounds__(256)
+k_ref_resid_band(const cplx* __restrict__ A, const XT* __restrict__ X, const double* __restrict__ W,
+                 cplx* __restrict__ Res, int n, int o) {
+    __shared__ cplx hs[16][32 + 1];   // hs[kk][rl] = H(r0 + rl, k(kk))
+    __shared__ cplx xs[16][64 + 1];   // xs[kk][cl] = X(k(kk), c0 + cl)
+    const int t = threadIdx.x, tr = t >> 4, tc = t & 15;
+    const size_t mat = blockIdx.z;
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 64;
+    const size_t nn = (size_t)n * n;
+    const cplx* Am = A + mat * nn;
+    const XT* Xm = X + mat * nn;
+    const int span = 32 + 2 * o;   // k(kk) = (r0 - o + kk) mod n, kk < span
+    cplx acc[2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = mk(0, 0);
+    for (int k0 = 0; k0 < span; k0 += 16) {
+        {   // H band: (kk, rl) = (t % 16, t / 16 + 16 h)
+            const int kk = t & 15;
+            const int kg = k0 + kk;
+            int k = r0 - o + kg;
+            k = k < 0 ? k + n : (k >= n ? k - n : k);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int rl = (t >> 4) + 16 * h, r = r0 + rl;
+                const int dist = kg - rl;   // k - r + o
+                cplx v = mk(0, 0);
+                if (kg < span && r < n && dist >= 0 && dist <= 2 * o) v = cconj(Am[(size_t)r * n + k]);
+                hs[kk][rl] = v;
+            }
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int cl = (t >> 4) + 16 * h, c = c0 + cl;
+                xs[kk][cl] = (kg < span && c < n) ? to_c64(Xm[(size_t)c * n + k]) : mk(0, 0);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            const cplx h0 = hs[kk][2 * tr], h1 = hs[kk][2 * tr + 1];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const cplx x = xs[kk][tc + 16 * j];
+                cfma(acc[0][j], h0, x);
+                cfma(acc[1][j], h1, x);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int c = c0 + tc + 16 * j;
+        if (c >= n) continue;
+        const double lam = W[mat * n + c];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r = r0 + 2 * tr + i;
+            if (r >= n) continue;
+            const size_t off = mat * nn + (size_t)c * n + r;
+            const cplx xr = to_c64(X[off]);
+            Res[off] = mk(acc[i][j].x - lam * xr.x, acc[i][j].y - lam * xr.y);
+        }
+    }
+}
 
 // Per eigenvector j (one warp each), in double: G_jj = x_j^H x_j, q_j = Re(x_j^H r_j) and
 // ||r_j||, stored as ST[3 (mat n + j) + {0, 1, 2}].
@@ -1903,6 +1990,7 @@ struct HeevPlan {
     int n;
     bool mixed;          // single-precision reduction + double refinement
     int refine_steps;    // mixed mode: 1 or 2
+    int band;            // >= 0: every matrix is a cyclic band of this half-bandwidth (rlm), else -1
     HetrdCfg hc;
     size_t smem_tri;
     bool small_bt;       // k_ormtr (register-resident Z chunk) or the blocked GEMM path
@@ -1914,10 +2002,11 @@ struct HeevPlan {
         off_y, off_mu, off_st, off_pv, per;
 };
 
-static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
+static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1) {
     HeevPlan p{};
     p.n = n;
     p.mixed = mixed;
+    p.band = band >= 0 && 32 + 2 * band <= n ? band : -1;   // the band residual needs 32 + 2o <= n
     p.refine_steps = mixed ? refine_steps : 0;
     const size_t ce = mixed ? sizeof(cplxf) : sizeof(cplx);   // working complex element
     p.npanels = n >= HT_BLOCKED_MIN ? (n - HT_TAIL + HP_W - 1) / HP_W : 0;
@@ -1964,6 +2053,15 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2) {
 
 // Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch (double precision).
 size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n, false).per; }
+
+// Largest chunk of matrices one heev_chunk call may take: the grid y / z extent (65535) of
+// the per-matrix launches, and of the (matrix, block) batches of the GEMM back-transformation.
+size_t heev_max_chunk(int n) {
+    const HeevPlan p = heev_plan(n, false);
+    size_t c = 65535;
+    if (!p.small_bt) c = std::min<size_t>(c, 65535 / std::max(p.nblk64, 1));
+    return c;
+}
 
 #define RLMB_CHUNK_LAUNCHED()                                     \
     do {                                                          \
@@ -2014,7 +2112,7 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
             RLMB_CHUNK_LAUNCHED();
             m -= HP_W;
             RLMB_CHUNK_PROF("k_hetrd");
-            if (launch_zgemm<C, 64>(st, OpPanelA<C>{PV, PWb, n}, OpPanelB<C>{PV, PWb, n}, EpHer2k<C>{A, n}, m, m,
+            if (launch_work_gemm<C, 64>(st, OpPanelA<C>{PV, PWb, n}, OpPanelB<C>{PV, PWb, n}, EpHer2k<C>{A, n}, m, m,
                                     2 * HP_W, nb) != cudaSuccess)
                 return RLMB_ERR_CUDA;
             RLMB_CHUNK_LAUNCHED();
@@ -2054,7 +2152,7 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         return RLMB_OK;
     }
     RLMB_CHUNK_PROF("k_larft");
-    if (launch_zgemm<C, 64>(st, OpBlkReflH<C>{Aw, n, p.nblk64}, OpBlkRefl<C>{Aw, n, p.nblk64},
+    if (launch_work_gemm<C, 64>(st, OpBlkReflH<C>{Aw, n, p.nblk64}, OpBlkRefl<C>{Aw, n, p.nblk64},
                             EpStore<C>{Tw, BT_NB, (size_t)BT_NB * BT_NB}, BT_NB, BT_NB, n, nb * p.nblk64) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
@@ -2076,12 +2174,12 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         const int i0 = j * BT_NB;
         const int rows = std::min(i0 + BT_NB - 1, n - 2) + 1;   // rows 0..i1 carry the block
         RLMB_CHUNK_PROF("k_ormtr");
-        if (launch_zgemm<C, 64>(st, OpReflH<C>{Aw, n, i0}, OpColB<C, C>{Xw, n, nn}, EpStore<C>{G, BT_NB, gs},
+        if (launch_work_gemm<C, 64>(st, OpReflH<C>{Aw, n, i0}, OpColB<C, C>{Xw, n, nn}, EpStore<C>{G, BT_NB, gs},
                                 BT_NB, n, rows, nb) != cudaSuccess)
             return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
         RLMB_CHUNK_PROF("k_ormtr");
-        if (launch_zgemm<C, 64>(st, OpRowA<C, C, false>{Tw + (size_t)j * BT_NB * BT_NB, BT_NB,
+        if (launch_work_gemm<C, 64>(st, OpRowA<C, C, false>{Tw + (size_t)j * BT_NB * BT_NB, BT_NB,
                                                         (size_t)p.nblk64 * BT_NB * BT_NB},
                                 OpColB<C, C>{G, BT_NB, gs}, EpStore<C>{W2, BT_NB, gs}, BT_NB, n, BT_NB, nb) != cudaSuccess)
             return RLMB_ERR_CUDA;
@@ -2089,7 +2187,7 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         RLMB_CHUNK_PROF("k_ormtr");
         // X -= V W': 64-row tiles (two CTAs per SM) on the DMMA engine, 128 in single precision
         constexpr int BMX = std::is_same<C, cplx>::value ? 64 : 128;
-        if (launch_zgemm<C, BMX>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs}, EpSub<C>{Xw, n},
+        if (launch_work_gemm<C, BMX>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs}, EpSub<C>{Xw, n},
                                  rows, n, BT_NB, nb) != cudaSuccess)
             return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
@@ -2099,15 +2197,18 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
 
 // One refinement step from the vectors X (single or double) to Out (double, not X).
 template <class XT>
-static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const cplx* A, const XT* X,
+static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int nb, const cplx* A, const XT* X,
                        double* W, cplx* Res, cplxf* F, int2* CL, cplx* YB, double* MU, double* ST,
                        cplx* Out, long long* launches) {
     const size_t nn = (size_t)n * n;
     const unsigned gw = (unsigned)(((size_t)nb * n + 7) / 8);   // one warp per column
     RLMB_CHUNK_PROF("k_ref_resid");
-    if (launch_zgemm<cplx, 64>(st, OpColA<cplx, cplx>{A, n, nn}, OpColB<cplx, XT>{X, n, nn}, EpResid<XT>{X, W, Res, n},
-                                n, n, n, nb) != cudaSuccess)
+    if (band >= 0) {   // cyclic band H: only 32 + 2 band rows of X per output tile
+        k_ref_resid_band<XT><<<dim3((n + 31) / 32, (n + 63) / 64, nb), 256, 0, st>>>(A, X, W, Res, n, band);
+    } else if (launch_zgemm<cplx, 64>(st, OpColA<cplx, cplx>{A, n, nn}, OpColB<cplx, XT>{X, n, nn},
+                                      EpResid<XT>{X, W, Res, n}, n, n, n, nb) != cudaSuccess) {
         return RLMB_ERR_CUDA;
+    }
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_colstats");
     k_ref_colstats<XT><<<gw, 256, 0, st>>>(X, Res, ST, n, nb);
@@ -2116,7 +2217,7 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const 
     k_ref_clusters<<<(nb + 127) / 128, 128, 0, st>>>(W, ST, CL, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_coupling");
-    if (launch_zgemm<cplx, 64>(st, OpRowA<cplx, XT, true>{X, n, nn}, OpColB<cplx, cplx>{Res, n, nn},
+    if (launch_zgemm_tc<cplx>(st, OpRowA<cplx, XT, true>{X, n, nn}, OpColB<cplx, cplx>{Res, n, nn},
                                 EpCoupling<XT>{X, W, CL, F, n}, n, n, n, nb) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
@@ -2135,7 +2236,7 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int nb, const 
     k_ref_diag<<<(unsigned)(((size_t)nb * n + 255) / 256), 256, 0, st>>>(ST, CL, W, F, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_update");
-    if (launch_zgemm<cplxf, 64>(st, OpColA<cplxf, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
+    if (launch_zgemm_tc<cplxf>(st, OpColA<cplx, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
                                  EpUpdate<XT>{X, Out, n}, n, n, n, nb) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
@@ -2212,11 +2313,12 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     // refinement: the single-precision copy of H is free now and holds F.  Step 1 starts
     // from the single-precision vectors, step 2 from step 1's double vectors (X1); the
     // last step writes the caller's buffer (every step's residual reads H first).
-    if (int rc = refine_step<cplxf>(ctx, st, n, nb, A, Xw, W, Res, As, CL, YB, MU, ST,
+    if (int rc = refine_step<cplxf>(ctx, st, n, p.band, nb, A, Xw, W, Res, As, CL, YB, MU, ST,
                                     p.refine_steps >= 2 ? X1 : A, launches))
         return rc;
     if (p.refine_steps >= 2)
-        if (int rc = refine_step<cplx>(ctx, st, n, nb, A, X1, W, Res, As, CL, YB, MU, ST, A, launches)) return rc;
+        if (int rc = refine_step<cplx>(ctx, st, n, p.band, nb, A, X1, W, Res, As, CL, YB, MU, ST, A, launches))
+            return rc;
     return RLMB_OK;
 }
 #undef RLMB_CHUNK_LAUNCHED
@@ -2231,12 +2333,14 @@ int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n,
 
 using namespace rlmb;
 
-extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch,
-                                  int* d_info) {
+// The batched eigensolve of rlmb_heevd_batched with a structure hint: band >= 0 declares every
+// matrix a cyclic band of that half-bandwidth (the rlm Hamiltonian), which the mixed mode's
+// refinement uses for its residual; band < 0 is a dense matrix.
+int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch, int* d_info, int band) {
     if (!ctx || !d_a || !d_w || n <= 0 || batch < 0) return RLMB_ERR_ARG;
     if (batch == 0) return RLMB_OK;
     RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
-    const HeevPlan plan = heev_plan(n, ctx->precision == RLMB_PRECISION_MIXED, ctx->refine_steps);
+    const HeevPlan plan = heev_plan(n, ctx->precision == RLMB_PRECISION_MIXED, ctx->refine_steps, band);
     const size_t per = plan.per;
     // workspace: 8 GB, or for large orders enough for two resident matrices per SM (one
     // CTA each in k_tridiag), capped at 60 % of the free memory
@@ -2248,6 +2352,7 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
     size_t budget = std::max<size_t>((size_t)8 << 30, 2 * 148 * per);
     budget = std::min<size_t>(budget, free_b / 10 * 6 + ctx->ws_bytes);
     budget = std::max<size_t>(budget, per);
+    if (ctx->frozen) budget = std::max<size_t>(per, ctx->ws_bytes);   // capture: the workspace as sized before
     size_t chunk = std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)batch));
     chunk = std::min<size_t>(chunk, 65535);   // grid y / z extent of the per-matrix launches
     if (!plan.small_bt) chunk = std::min<size_t>(chunk, 65535 / std::max(plan.nblk64, 1));   // (matrix, block) batches
@@ -2263,5 +2368,44 @@ extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, i
                                 d_info ? d_info + b0 : nullptr, nb, ctx->ws, &unused))
             return rc;
     }
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch, int* d_info) {
+    return rlmb::heevd_batched_band(ctx, d_a, d_w, n, batch, d_info, -1);
+}
+
+// Batched complex GEMM C = A B (column-major complex128, A m x k, B k x n, C m x n, matrices
+// packed back to back) on either engine: the FP64 tensor path (DMMA) or the tcgen05 TF32
+// tensor cores with split operands (FP32-class accuracy).
+extern "C" int rlmb_zgemm_batched(rlmb_context* ctx, const double* d_a, const double* d_b, double* d_c, int m,
+                                  int n, int k, int batch, int engine) {
+    if (!ctx || !d_a || !d_b || !d_c || m <= 0 || n <= 0 || k < 0 || batch < 0 ||
+        (engine != RLMB_GEMM_FP64 && engine != RLMB_GEMM_TF32X3))
+        return RLMB_ERR_ARG;
+    if (batch == 0) return RLMB_OK;
+    if (batch > 65535) return RLMB_ERR_ARG;
+    RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
+    const cplx* A = reinterpret_cast<const cplx*>(d_a);
+    const cplx* B = reinterpret_cast<const cplx*>(d_b);
+    cplx* Cm = reinterpret_cast<cplx*>(d_c);
+    const OpColA<cplx, cplx> la{A, m, (size_t)m * k};
+    const OpColB<cplx, cplx> lb{B, k, (size_t)k * n};
+    const EpStore<cplx> ep{Cm, m, (size_t)m * n};
+    prof_begin(ctx, engine == RLMB_GEMM_FP64 ? "k_zgemm_dmma" : "k_zgemm_tc");
+    const cudaError_t e = engine == RLMB_GEMM_FP64 ? launch_zgemm<cplx, 64>(ctx->stream, la, lb, ep, m, n, k, batch)
+                                                   : launch_zgemm_tc<cplx>(ctx->stream, la, lb, ep, m, n, k, batch);
+    prof_end(ctx);
+    ctx->launches++;
+    return e == cudaSuccess ? RLMB_OK : RLMB_ERR_CUDA;
+}
+
+// Number of tcgen05 GEMM tiles whose bounded mbarrier waits ran out since the library was
+// loaded on the current device (synchronises the device).
+extern "C" int rlmb_tc_fault_count(rlmb_context* ctx, int* count) {
+    if (!ctx || !count) return RLMB_ERR_ARG;
+    RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
+    RLMB_CUDA_TRY(cudaDeviceSynchronize());
+    RLMB_CUDA_TRY(cudaMemcpyFromSymbol(count, g_tc_fault, sizeof(int)));
     return RLMB_OK;
 }

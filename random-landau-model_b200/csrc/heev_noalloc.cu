@@ -4,14 +4,17 @@
 // reserved in full by another allocator (a framework's caching pool, or a job running
 // under a fixed device-memory budget), and callers that must not take cudaMalloc /
 // cudaFree's implicit device synchronisation in the middle of their own work.  For them
-// rlmb_heevd_batched_noalloc runs the same kernels as rlmb_heevd_batched, but on scratch
-// that lives in the file-scope device array below instead of a context workspace.
+// rlmb_heevd_batched_noalloc runs the double-precision kernels of rlmb_heevd_batched (always
+// FP64, never the mixed mode's refinement, whatever precision other callers' contexts use),
+// but on scratch that lives in the file-scope device array below instead of a context
+// workspace.
 #include <mutex>
 
 #include "common.cuh"
 
 namespace rlmb {
 size_t heev_scratch_bytes_per_matrix(int n);
+size_t heev_max_chunk(int n);
 int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n, int nb,
                           void* scratch, long long* launches);
 }  // namespace rlmb
@@ -62,10 +65,28 @@ extern "C" int rlmb_heevd_batched_noalloc(double* d_a, double* d_w, int n, int b
         return RLMB_ERR_TOO_LARGE;
     }
     if (batch == 0) return RLMB_OK;
+    // a launch error the caller left pending is reported, not consumed (this call's own
+    // launch checks would otherwise take it as theirs)
+    if (cudaPeekAtLastError() != cudaSuccess) return RLMB_ERR_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the scratch address is the current device's: the stream must belong to that device
+    if (st) {
+        int cur = 0, sdev = 0;
+        if (cudaGetDevice(&cur) != cudaSuccess || cudaStreamGetDevice(st, &sdev) != cudaSuccess) return RLMB_ERR_CUDA;
+        if (sdev != cur) {
+            fprintf(stderr, "rlmb_heevd_batched_noalloc: the stream belongs to device %d, the current device is %d\n",
+                    sdev, cur);
+            return RLMB_ERR_ARG;
+        }
+    }
     void* scratch = nullptr;
     if (int rc = scratch_address(&scratch)) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int chunk = (int)std::min<size_t>((size_t)batch, RLMB_NOALLOC_SCRATCH_BYTES / per);
+    // chunks: as many matrices as the array holds, within the grid limits of the per-matrix
+    // launches, and equal in size (a short last chunk would leave most SMs idle)
+    size_t cap = std::min<size_t>((size_t)batch, RLMB_NOALLOC_SCRATCH_BYTES / per);
+    cap = std::max<size_t>(1, std::min(cap, rlmb::heev_max_chunk(n)));
+    const size_t nchunks = ((size_t)batch + cap - 1) / cap;
+    const int chunk = (int)(((size_t)batch + nchunks - 1) / nchunks);
     long long launches = 0;
     const size_t nn = (size_t)n * n;
     for (int b0 = 0; b0 < batch; b0 += chunk) {

@@ -606,7 +606,7 @@ __device__ __forceinline__ cplx link_dir(const cplx* __restrict__ S, const cplx*
 }
 
 __device__ void build_link_S(cplx* S, cplx* Dtab, const cplx* __restrict__ ha, const cplx* __restrict__ hbb,
-                             int N, int L, int ly, int Lxp, int Q, int dir, double shift) {
+                             int N, int L, int ly, int Lxp, int Q, int dir, double shift, bool transposed = false) {
     for (int dlt = threadIdx.x; dlt < L; dlt += blockDim.x) {
         // D_L(dlt + shift) = sum_j e^{i 2pi (dlt + shift) j / L}, dlt = index difference mod L
         cplx acc = mk(0, 0);
@@ -627,7 +627,7 @@ __device__ void build_link_S(cplx* S, cplx* Dtab, const cplx* __restrict__ ha, c
         else { b = kxa * ly + l; dlt = (kya - l + ly) % ly; }
         cplx ov = mk(0, 0);
         for (int q = 0; q < Q; ++q) cfmac(ov, ha[(size_t)a * Q + q], hbb[(size_t)b * Q + q]);
-        S[idx] = cscale(cmul(Dtab[dlt], ov), pref);
+        S[transposed ? (size_t)l * N + a : (size_t)idx] = cscale(cmul(Dtab[dlt], ov), pref);
     }
 }
 
@@ -666,9 +666,76 @@ k_hlm_links(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int
     }
 }
 
+// The same links with one warp per state n: the warp stages rows n of the two neighbours'
+// eigenvector matrices in shared memory, its lanes walk the Bloch index a of row n of its own
+// matrix (coalesced 16-byte loads of all three rows), and the S blocks are stored transposed
+// (S[l][a]) so that consecutive lanes read consecutive words.  Per-lane partial overlaps are
+// reduced across the warp.
 template <int L1, int L2>
-static int launch_links_t(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,
-                          int nsamples, cplx* U1, cplx* U2) {
+__global__ void __launch_bounds__(256)
+k_hlm_links_w(const cplx* __restrict__ hb, const cplx* __restrict__ X, int lx, int ly, int Q, int g,
+              cplx* __restrict__ U1, cplx* __restrict__ U2) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int Lxp = lx / Q, N = Lxp * ly;
+    const int kpts = (g + 1) * g;
+    const int job = blockIdx.x, sample = job / kpts, t = job % kpts;
+    const int t1 = t / g, t2 = t % g;
+    cplx* T1 = reinterpret_cast<cplx*>(smem_raw);      // theta_1 link, transposed: T1[l][a]
+    cplx* T2 = T1 + (size_t)N * L1;                      // theta_2 link, T2[l][a]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    cplx* r1 = T2 + (size_t)N * L2 + (size_t)w * 2 * N;   // this warp's two staged rows
+    cplx* r2 = r1 + N;
+    __shared__ cplx Dtab[LINK_MAXL];
+    const bool has1 = t1 < g;
+    const int t2n = t2 + 1 == g ? 0 : t2 + 1;            // theta_2 = g is the copy of theta_2 = 0
+    const cplx* ha = hb + ((size_t)t1 * (g + 1) + t2) * N * Q;
+    if (has1) {
+        build_link_S(T1, Dtab, ha, hb + ((size_t)(t1 + 1) * (g + 1) + t2) * N * Q, N, L1, ly, Lxp, Q, 0,
+                     -1.0 / g, true);
+        __syncthreads();
+    }
+    build_link_S(T2, Dtab, ha, hb + ((size_t)t1 * (g + 1) + t2n) * N * Q, N, L2, ly, Lxp, Q, 1,
+                 (double)(t2 - t2n) / g, true);
+    __syncthreads();
+    const size_t nn = (size_t)N * N;
+    const cplx* Xa = X + ((size_t)sample * kpts + t) * nn;
+    const cplx* Xb1 = X + ((size_t)sample * kpts + (t1 + 1) * g + t2) * nn;
+    const cplx* Xb2 = X + ((size_t)sample * kpts + t1 * g + t2n) * nn;
+    for (int n = w; n < N; n += blockDim.x >> 5) {
+        for (int b = lane; b < N; b += 32) {
+            if (has1) r1[b] = Xb1[(size_t)n * N + b];
+            r2[b] = Xb2[(size_t)n * N + b];
+        }
+        __syncwarp();
+        cplx acc1 = mk(0, 0), acc2 = mk(0, 0);
+        for (int a = lane; a < N; a += 32) {
+            const int kxa = a / ly, kya = a % ly;
+            const cplx ua = Xa[(size_t)n * N + a];
+            if (has1) {   // theta_1 link: partners b = l * ly + kya
+                cplx y = mk(0, 0);
+#pragma unroll
+                for (int l = 0; l < L1; ++l) cfma(y, T1[(size_t)l * N + a], r1[l * ly + kya]);
+                cfmac(acc1, ua, y);
+            }
+            cplx y = mk(0, 0);   // theta_2 link: partners b = kxa * ly + l
+#pragma unroll
+            for (int l = 0; l < L2; ++l) cfma(y, T2[(size_t)l * N + a], r2[kxa * ly + l]);
+            cfmac(acc2, ua, y);
+        }
+        acc1 = warp_sum(acc1);
+        acc2 = warp_sum(acc2);
+        if (lane == 0) {
+            const size_t o = ((size_t)sample * kpts + t) * N + n;
+            if (has1) U1[o] = acc1;
+            U2[o] = acc2;
+        }
+        __syncwarp();   // the staged rows are rewritten for the next state
+    }
+}
+
+template <int L1, int L2>
+static int launch_links_thread(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,
+                               int nsamples, cplx* U1, cplx* U2) {
     const int N = lx * ly / Q;
     const size_t smem = (size_t)N * (L1 + L2) * sizeof(cplx);
     if (smem > 220 * 1024) return RLMB_ERR_ARG;
@@ -678,6 +745,24 @@ static int launch_links_t(rlmb_context* ctx, const cplx* hb, const cplx* X, int 
     k_hlm_links<L1, L2><<<nsamples * (g + 1) * g, 256, smem, ctx->stream>>>(hb, X, lx, ly, Q, g, U1, U2);
     RLMB_LAUNCHED(ctx);
     return RLMB_OK;
+}
+
+// Warp-per-state links where their shared memory fits (the transposed S blocks and two
+// staged rows per warp), else the thread-per-state kernel.
+template <int L1, int L2>
+static int launch_links_t(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,
+                          int nsamples, cplx* U1, cplx* U2) {
+    const int N = lx * ly / Q;
+    const size_t smem_w = ((size_t)N * (L1 + L2) + (size_t)8 * 2 * N) * sizeof(cplx);
+    if (smem_w <= 220 * 1024) {
+        RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hlm_links_w<L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_w));
+        prof_begin(ctx, "k_hlm_links");
+        k_hlm_links_w<L1, L2><<<nsamples * (g + 1) * g, 256, smem_w, ctx->stream>>>(hb, X, lx, ly, Q, g, U1, U2);
+        RLMB_LAUNCHED(ctx);
+        return RLMB_OK;
+    }
+    return launch_links_thread<L1, L2>(ctx, hb, X, lx, ly, Q, g, nsamples, U1, U2);
 }
 
 int launch_hlm_links(rlmb_context* ctx, const cplx* hb, const cplx* X, int lx, int ly, int Q, int g,

@@ -18,6 +18,8 @@ int launch_plaquettes(rlmb_context* ctx, const cplx* U1, const cplx* U2, const d
                       int g, int nsamples, int hlm, double* energies, double* chern);
 int launch_fhs_line(rlmb_context* ctx, const cplx* prev, const cplx* cur, int n_phi, int dim_vec,
                     int g, double* out);
+int launch_rlm_disorder_at(rlmb_context* ctx, int nimp, double L1, double L2, unsigned long seed,
+                           const int* d_sample0, int offset, int count, double* d_x, double* d_y, double* d_s);
 // hlm
 int launch_hlm_bloch(rlmb_context* ctx, int lx, int ly, int Q, int band, int g, int t1_0, int t1_1,
                      int t2_0, int t2_1, cplx* hb);

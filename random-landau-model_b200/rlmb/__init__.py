@@ -37,6 +37,9 @@ _SIGNATURES = {
     "rlmb_heevd_batched": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "rlmb_heevd_host": (ctypes.c_int, [_vp, _c_dp, _c_dp, ctypes.c_int, ctypes.c_int]),
     "rlmb_heevd_batched_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "rlmb_zgemm_batched": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int]),
+    "rlmb_tc_fault_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "rlmb_rlm_coeff_tables": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double, _c_dp, _c_dp, _c_dp]),
     "rlmb_rlm_disorder": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulong,
@@ -54,6 +57,16 @@ _SIGNATURES = {
     "rlmb_rlm_mesh_solve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_int, ctypes.c_ulong, ctypes.c_int, ctypes.c_int,
                                            _c_dp, _c_dp]),
+    "rlmb_rlm_mesh_solve_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                  ctypes.c_int, ctypes.c_ulong, ctypes.c_int, ctypes.c_int,
+                                                  _vp, _vp]),
+    "rlmb_rlm_fss_graph_create": (ctypes.c_int, [ctypes.c_int, _c_ip, ctypes.c_int, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_int, ctypes.c_ulong, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.POINTER(_vp)]),
+    "rlmb_rlm_fss_graph_launch": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "rlmb_rlm_fss_graph_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "rlmb_rlm_fss_graph_results": (ctypes.c_int, [_vp, ctypes.c_int, _c_dp, _c_dp]),
+    "rlmb_rlm_fss_graph_destroy": (ctypes.c_int, [_vp]),
     "rlmb_rlm_mesh_export": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              ctypes.c_ulong, ctypes.c_int, ctypes.c_char_p, _c_dp, _c_dp]),
     "rlmb_rlm_disorder_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulong,
@@ -138,7 +151,7 @@ def rlm_disorder(impurity_num, L1, L2, seed, sample):
 
 
 def hlm_potentials(seed, n_sites, n_sample):
-    """[n_sample, n_sites] on-site potentials of hlm/main_hlm_cpu.cpp:345-358."""
+    """[n_sample, n_sites] on-site potentials of hlm/main_hlm_cpu.cpp:66-67,79."""
     out = np.zeros((n_sample, n_sites))
     _check(lib().rlmb_hlm_potentials(seed, n_sites, n_sample, _dp(out)), "hlm_potentials")
     return out
@@ -233,6 +246,28 @@ class Context:
             _check(rc, "rlmb_heevd_batched")
         return w
 
+    GEMM_FP64, GEMM_TF32X3 = 0, 1
+
+    def zgemm(self, at, bt, engine=GEMM_TF32X3):
+        """C = A B for torch complex128 CUDA tensors at[batch, k, m] = A^T and bt[batch, n, k] =
+        B^T (the column-major matrices); returns ct[batch, n, m] = C^T."""
+        import torch
+        assert at.is_cuda and bt.is_cuda and at.dtype == bt.dtype == torch.complex128
+        assert at.is_contiguous() and bt.is_contiguous()
+        batch, k, m = at.shape
+        n = bt.shape[1]
+        assert bt.shape == (batch, n, k)
+        ct = torch.empty((batch, n, m), dtype=torch.complex128, device=at.device)
+        self.sync_stream()
+        _check(lib().rlmb_zgemm_batched(self.h, _ptr(at), _ptr(bt), _ptr(ct), m, n, k, batch, int(engine)),
+               "rlmb_zgemm_batched")
+        return ct
+
+    def tc_fault_count(self):
+        c = ctypes.c_int()
+        _check(lib().rlmb_tc_fault_count(self.h, ctypes.byref(c)), "rlmb_tc_fault_count")
+        return c.value
+
     def mkl_heevd(self, h, n):
         """Drop-in for diag_wrappers/mkl_diag.cpp:2-9 on a host buffer of n*n complex
         (col-major, 'U'): overwrites h with eigenvectors, returns eigenvalues."""
@@ -318,6 +353,16 @@ class Context:
         _check(rc, "rlmb_rlm_mesh_solve")
         return e, c
 
+    def rlm_mesh_solve_device(self, n_phi, quanta_concentration, impurity_concentration, n_mesh, seed, sample0,
+                              d_energies, d_chern):
+        """rlm_mesh_solve into torch float64 CUDA tensors [n_samples, n_phi] (results stay on
+        the device)."""
+        self.sync_stream()
+        rc = lib().rlmb_rlm_mesh_solve_device(self.h, n_phi, quanta_concentration, impurity_concentration, n_mesh,
+                                              seed, sample0, d_energies.shape[0], _ptr(d_energies), _ptr(d_chern))
+        self.last_failures = max(rc, 0)
+        _check(rc, "rlmb_rlm_mesh_solve_device")
+
     def rlm_disorder_device(self, impurity_num, L1, L2, seed, sample0, count):
         """(x, y, s) torch float64 CUDA tensors [count, impurity_num] drawn on the device."""
         import torch
@@ -367,3 +412,49 @@ class Context:
                                               d_potentials.shape[0], _ptr(d_energies), _ptr(d_chern))
         self.last_failures = max(rc, 0)
         _check(rc, "rlmb_hlm_mesh_solve_device")
+
+
+class FssGraph:
+    """Several rlm orders solved by one CUDA graph launch per step (rlmb_rlm_fss_graph_*):
+    every launch solves samples sample0 .. sample0+n_samples-1 of each order in n_phis, the
+    orders on concurrent branches of the graph."""
+
+    def __init__(self, device, n_phis, quanta_concentration=1.0, impurity_concentration=16.0, n_mesh=16, seed=1,
+                 n_samples=16, precision=0):
+        self.n_phis = [int(n) for n in n_phis]
+        self.n_samples = int(n_samples)
+        arr = (ctypes.c_int * len(self.n_phis))(*self.n_phis)
+        h = ctypes.c_void_p()
+        _check(lib().rlmb_rlm_fss_graph_create(device, arr, len(self.n_phis), quanta_concentration,
+                                               impurity_concentration, n_mesh, seed, self.n_samples, int(precision),
+                                               ctypes.byref(h)), "rlmb_rlm_fss_graph_create")
+        self.h = h
+
+    def launch(self, sample0):
+        _check(lib().rlmb_rlm_fss_graph_launch(self.h, int(sample0)), "rlmb_rlm_fss_graph_launch")
+
+    def stream(self):
+        """The graph's stream as a torch ExternalStream (for CUDA-event timing)."""
+        import torch
+        st = ctypes.c_void_p()
+        _check(lib().rlmb_rlm_fss_graph_stream(self.h, ctypes.byref(st)), "rlmb_rlm_fss_graph_stream")
+        return torch.cuda.ExternalStream(st.value)
+
+    def results(self, index):
+        """(energies, chern) [n_samples, n_phi] of order index from the last launch."""
+        n = self.n_phis[index]
+        e = np.zeros((self.n_samples, n))
+        c = np.zeros((self.n_samples, n))
+        _check(lib().rlmb_rlm_fss_graph_results(self.h, index, _dp(e), _dp(c)), "rlmb_rlm_fss_graph_results")
+        return e, c
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().rlmb_rlm_fss_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -355,8 +355,50 @@ def test_rlm_disorder_device_matches_host(ctx, nimp, samples):
         assert np.array_equal(x[k], hx) and np.array_equal(y[k], hy) and np.array_equal(s[k], hs)
 
 
+@pytest.mark.parametrize("nimp", [256, 4096, 48000])
+def test_rlm_disorder_device_continuation_matches_host(ctx, nimp):
+    """Consecutive calls continue the context's saved MT19937 stream (one CTA draws the samples
+    in order) instead of skipping ahead per sample: the draws are still the host stream's,
+    bit for bit, including calls whose boundary falls inside a 624-output block, a call that
+    jumps back (fresh skip), and a call that resumes after it."""
+    import rlmb
+    L = float(np.sqrt(nimp / 16.0))
+    for lo, cnt in ((0, 2), (2, 3), (5, 1), (1, 2), (3, 2)):
+        x, y, s = (t.cpu().numpy() for t in ctx.rlm_disorder_device(nimp, L, L, 7, lo, cnt))
+        for k in range(cnt):
+            hx, hy, hs = rlmb.rlm_disorder(nimp, L, L, 7, lo + k)
+            assert np.array_equal(x[k], hx) and np.array_equal(y[k], hy) and np.array_equal(s[k], hs)
+
+
 def test_hlm_potentials_device_matches_host(ctx):
     import rlmb
     host = rlmb.hlm_potentials(1, 768, 70)
     dev = ctx.hlm_potentials_device(1, 768, 3, 67).cpu().numpy()
     assert np.array_equal(dev, host[3:70])
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fss_graph_matches_mesh_solve(ctx, precision):
+    """Several orders in one captured CUDA graph, replayed for two sample blocks: every order's
+    energies and Chern numbers equal the plain mesh solve of the same samples, and order 64
+    sample 0 matches the reference fixture."""
+    import rlmb
+    sizes = (16, 48, 64)
+    fg = rlmb.FssGraph(0, sizes, 1.0, 16.0, 4, 3, 2, precision)
+    ctx.precision = precision
+    try:
+        for s0 in (0, 2):
+            fg.launch(s0)
+            for i, n in enumerate(sizes):
+                e, c = fg.results(i)
+                er, cr = ctx.rlm_mesh_solve(n, 1.0, 16.0, 4, 3, s0, 2)
+                assert np.abs(e - er).max() <= 1e-12 * np.abs(er).max()
+                assert np.array_equal(np.rint(c), np.rint(cr)) and np.abs(c - cr).max() < 1e-9
+        fg.launch(0)
+        d = golden("rlm_n64_g4_c1_s3.npz")
+        e, c = fg.results(2)
+        assert np.abs(e[0] - d["energies"][0]).max() <= 1e-10 * np.abs(d["energies"][0]).max()
+        assert np.array_equal(np.rint(c[0]), np.rint(d["chern"][0]))
+    finally:
+        ctx.precision = 0
+        fg.close()

@@ -2,9 +2,11 @@
 
 rlmb_heevd_batched_noalloc serves callers that cannot allocate device memory (device
 memory already reserved in full by another allocator, or no tolerance for cudaMalloc's
-implicit synchronisation mid-run): its scratch is a fixed file-scope device array.  Its
-results must match rlmb_heevd_batched's, call after call, since every call reuses the same
-array.  This file is collected last so that a failure here leaves the other tests run.
+implicit synchronisation mid-run): its scratch is a fixed file-scope device array.  Every
+call is checked on its own against numpy (eigenvalues, residual, orthogonality, with the
+tolerances of test_gpu_parity._check_eig) and against rlmb_heevd_batched on the same
+inputs, call after call, since every call reuses the same array.  This file is collected
+last so that a failure here leaves the other tests run.
 """
 import ctypes
 
@@ -46,6 +48,20 @@ def _run_noalloc(lib, a0):
     return w.cpu().numpy(), a.cpu().numpy()
 
 
+def _check_eig(a0, w, X):
+    """Eigenpairs of each column-major matrix a0[b] (stored transposed: a0[b] = M^T) against
+    numpy: eigenvalues vs eigvalsh, residual ||M X - X diag(w)||_F and ||X^H X - I||_F."""
+    for b in range(a0.shape[0]):
+        M = a0[b].T
+        Xb = X[b].T   # column k = eigenvector k
+        wref = np.linalg.eigvalsh(M)
+        scale = np.abs(wref).max()
+        assert np.abs(w[b] - wref).max() <= 1e-12 * scale
+        nrm = np.linalg.norm(M)
+        assert np.linalg.norm(M @ Xb - Xb * w[b][None, :]) <= 1e-12 * nrm
+        assert np.linalg.norm(Xb.conj().T @ Xb - np.eye(M.shape[0])) <= 1e-11
+
+
 def _same(wa, Xa, wb, Xb):
     scale = np.abs(wa).max()
     assert np.abs(wa - wb).max() <= EIG_TOL * scale
@@ -66,6 +82,7 @@ def test_noalloc_matches_batched_twice(n, batch):
         a0 = _hermitian_batch(rng, batch, n)
         wb, Xb = _run_batched(ctx, a0)
         wn, Xn = _run_noalloc(lib, a0)
+        _check_eig(a0, wn, Xn)
         _same(wb, Xb, wn, Xn)
     ctx.close()
 
