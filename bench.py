@@ -777,9 +777,12 @@ FSS_SIZES = (64, 128, 192, 256, 384, 512)
 
 def run_gpu_fss(args):
     """Finite-size-scaling workload: rlm with n_phi in FSS_SIZES, 16 samples each, g=16,
-    impurity concentration 16 -- one rlmb_rlm_mesh_solve call per size per step (FP64).
-    Reports k-point solves/s per size and for the whole step, and each size's eigensolver
-    throughput against the FP64 roofline (13.33 n^3 flops per solve)."""
+    impurity concentration 16, FP64.  Two forms of the same work: one rlmb_rlm_mesh_solve call
+    per size per step (sizes one after another), and one CUDA-graph launch per step that runs
+    every size on its own concurrent branch (rlmb_rlm_fss_graph_*).  Reports k-point solves/s
+    per size (sequential form) and for the whole step in both forms, and each size's
+    eigensolver throughput against the FP64 roofline (13.33 n^3 flops per solve)."""
+    import numpy as np
     import torch
     import rlmb
     ws, rank, local = _dist()
@@ -791,14 +794,15 @@ def run_gpu_fss(args):
     ctx = rlmb.Context(local)
     peak = ctx.fp64_peak_tflops()
     per = {}
+    seq_res = {}
     for n in FSS_SIZES:
         for _ in range(args.warmup):
-            ctx.rlm_mesh_solve(n, 1.0, 16.0, g, SEED, 0, ns)
+            ctx.rlm_mesh_solve(n, 1.0, 16.0, g, SEED, ns, ns)
         ctx.profile(True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for st in range(args.steps):
-            ctx.rlm_mesh_solve(n, 1.0, 16.0, g, SEED, ns * (st + 1), ns)
+            seq_res[n] = ctx.rlm_mesh_solve(n, 1.0, 16.0, g, SEED, 0, ns)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         prof = ctx.profile_report()
@@ -808,16 +812,41 @@ def run_gpu_fss(args):
         eig_tf = 13.33 * n ** 3 * solves / (eig_ms * 1e-3) / 1e12
         per[str(n)] = {"solves_per_s": solves / dt, "ms_per_step": 1e3 * dt / args.steps,
                        "eigensolve_tflops": eig_tf, "eigensolve_frac_of_fp64_peak": eig_tf / peak}
+    ctx.close()
     total_solves = len(FSS_SIZES) * ns * kpts * args.steps
-    total_s = sum(v["ms_per_step"] for v in per.values()) * args.steps / 1e3
-    line = {"metric": METRIC, "value": total_solves / total_s, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+    seq_s = sum(v["ms_per_step"] for v in per.values()) * args.steps / 1e3
+    # one graph launch per step, all sizes concurrent
+    fg = rlmb.FssGraph(local, FSS_SIZES, 1.0, 16.0, g, SEED, ns, 0)
+    st = fg.stream()
+    for _ in range(args.warmup):
+        fg.launch(0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        fg.launch(0)
+    e1.record(st)
+    torch.cuda.synchronize()
+    graph_ms = e0.elapsed_time(e1) / args.steps
+    same = True
+    for i, n in enumerate(FSS_SIZES):
+        e, c = fg.results(i)
+        er, cr = seq_res[n]
+        same = same and bool(np.array_equal(np.rint(c), np.rint(cr))) and \
+            bool(np.abs(e - er).max() <= 1e-12 * np.abs(er).max())
+    fg.close()
+    graph_value = len(FSS_SIZES) * ns * kpts / (graph_ms * 1e-3)
+    line = {"metric": METRIC, "value": graph_value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": graph_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "rlm finite-size scaling: n_phi in " + ",".join(map(str, FSS_SIZES)) +
                                    f", {ns} samples each per step, g={g}, impurity concentration 16, seed {SEED}",
-                       "api": "rlmb_rlm_mesh_solve per size (sizes run one after another)"},
+                       "api": "one rlmb_rlm_fss_graph_launch per step (value); rlmb_rlm_mesh_solve per size "
+                              "(sequential)"},
+            "graph": {"launches_per_step": 1, "ms_per_step": graph_ms, "solves_per_s": graph_value,
+                      "results_identical_to_sequential": same},
+            "sequential": {"ms_per_step": 1e3 * seq_s / args.steps, "solves_per_s": total_solves / seq_s},
             "per_size": per, "fp64_peak_tflops": peak}
-    ctx.close()
     print(json.dumps(line), flush=True)
 
 
@@ -853,9 +882,24 @@ def run_probe(args):
     if args.probe == "rlm":
         if args.mixed:
             ctx.precision = ctx.MIXED
-        ctx.rlm_mesh_solve(n, 1.0, 16.0, 4, SEED, 0, b)
+        ctx.rlm_mesh_solve(n, 1.0, 16.0, 4 if n > 1024 else 16, SEED, 0, b)
         torch.cuda.synchronize()
         print(json.dumps({"probe": "rlm", "n": n, "samples": b, "launches": ctx.launches}))
+        return
+    if args.probe == "hlm":
+        pots = rlmb.hlm_potentials(SEED, N_SITES, b)
+        ctx.hlm_mesh_solve(LX, LY, Q, BAND, G, pots)
+        torch.cuda.synchronize()
+        print(json.dumps({"probe": "hlm", "samples": b, "launches": ctx.launches}))
+        return
+    if args.probe == "fhs":
+        # one line pair of the reference layout at the hlm benchmark geometry
+        prev = torch.randn((G + 1, N_PHI, N_SITES), dtype=torch.complex128, device="cuda")
+        cur = torch.randn((G + 1, N_PHI, N_SITES), dtype=torch.complex128, device="cuda")
+        for _ in range(3):
+            ctx.fhs_line(prev, cur)
+        torch.cuda.synchronize()
+        print(json.dumps({"probe": "fhs", "n_phi": N_PHI, "dim_vec": N_SITES, "g": G}))
         return
     if args.mixed:
         ctx.precision = ctx.MIXED
@@ -879,7 +923,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision measurement on the same inputs")
     ap.add_argument("--mixed", action="store_true", help="probe in the mixed-precision mode")
-    ap.add_argument("--probe", default=None, choices=["heevd", "tcgemm", "rlm"],
+    ap.add_argument("--probe", default=None, choices=["heevd", "tcgemm", "rlm", "hlm", "fhs"],
                     help="run one small eigensolver batch only (for profiler captures)")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=296)

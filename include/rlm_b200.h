@@ -69,6 +69,21 @@ int rlmb_get_precision(const rlmb_context* ctx);
  * level.  Eigenvalues are within ~1e-11 relative after one step. */
 int rlmb_set_refinement_steps(rlmb_context* ctx, int steps);
 
+/* Eigensolver launch choices (no counterpart in the reference, whose solver is a library
+ * call).  With autotuning on, the first eigensolve of each order n in 64..1024 and precision
+ * mode on the context times every feasible configuration -- unblocked or blocked reduction,
+ * 256- or 512-thread panels, register-resident or GEMM back-transformation, 64- or 128-row
+ * tiles of the double-precision X update -- on copies of up to 2 x SMs of the call's own
+ * matrices and keeps the fastest for later calls of that order.  rlmb_heev_config reports the
+ * configuration used for (n, precision) (the tuned one, or the built-in one) and returns 1 if
+ * it was tuned or set, 0 if built-in; rlmb_set_heev_config pins one (-1 / 0 = built-in choice
+ * for that item).  panel_threads 0 means the built-in choice. */
+int rlmb_set_autotune(rlmb_context* ctx, int on);
+int rlmb_heev_config(rlmb_context* ctx, int n, int precision, int* blocked, int* gemm_bt, int* panel_threads,
+                     int* x_tile, double* ms_per_matrix);
+int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int blocked, int gemm_bt, int panel_threads,
+                         int x_tile);
+
 /* ------------------------------------------------- (b) Hermitian eigensolver
  * Batched full eigendecomposition, double precision, in place.
  * Replaces: mkl_heevd            diag_wrappers/mkl_diag.cpp:2-9   (host, col-major, 'U')
@@ -197,7 +212,8 @@ int rlmb_rlm_mesh_export(rlmb_context* ctx, int n_phi, double quanta_concentrati
 /* Several rlm orders in ONE CUDA graph launch per step (the finite-size-scaling batch; no
  * counterpart in the reference, whose driver runs one n_phi per process).  create prepares
  * the pipeline of each order n_phi[0..count) (its own stream and buffers, every buffer sized
- * by one uncaptured run of samples 0 .. n_samples-1) and captures all of them, one concurrent
+ * and the eigensolver configuration autotuned by one uncaptured run of samples
+ * 0 .. n_samples-1) and captures all of them, one concurrent
  * branch per order, in precision mode `precision` (RLMB_PRECISION_FP64 or _MIXED).  launch
  * queues one step -- samples sample0 .. sample0+n_samples-1 of every order -- on the graph's
  * stream (stream returns it, a cudaStream_t) without synchronising; results synchronises and

@@ -188,6 +188,7 @@ int rlmb_destroy(rlmb_context* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     prof_free(ctx);
+    tune_free(ctx);
     if (ctx->ws) cudaFree(ctx->ws);
     if (ctx->pipe) cudaFree(ctx->pipe);
     if (ctx->io) cudaFree(ctx->io);
@@ -580,7 +581,8 @@ static int rlm_mesh(rlmb_context* ctx, int n_phi, double qc, double ic, int n_me
 // plaquettes, device-side failure tally) on its context stream, and joins them.  The orders
 // run concurrently on the device: the small ones fill the SMs the large ones leave idle.
 // The first sample of a launch is written to device memory just before the graph runs, and
-// the disorder kernels read it there.
+// the disorder kernels read it there.  Each order's eigensolver launch configuration is
+// autotuned (rlmb_set_autotune) during its set-up run.
 struct FssOrder {
     rlmb_context* ctx;
     RlmPlan plan;
@@ -668,6 +670,7 @@ int rlmb_rlm_fss_graph_create(int device, const int* n_phi, int count, double qc
         }
         o.ctx->stream = st;
         o.ctx->precision = precision;
+        o.ctx->autotune = 1;   // the set-up run tunes this order's eigensolver configuration
         if (cudaMalloc(reinterpret_cast<void**>(&o.d_e), 2 * (size_t)n_samples * n_phi[i] * sizeof(double)) != cudaSuccess)
             return fail(RLMB_ERR_ALLOC);
         if ((rc = rlm_prepare(o.ctx, n_phi[i], qc, ic, n_mesh, seed, n_samples, &o.plan))) return fail(rc);

@@ -127,6 +127,9 @@ struct rlmb_context {
     uint32_t* mt_state;
     // set while a stream capture records this context's work: buffers may not grow then
     int frozen;
+    // eigensolver autotuning (rlmb_set_autotune) and its per-(order, precision) choices
+    int autotune;
+    void* tune;
     int mt_valid;
     unsigned long mt_seed;
     int mt_nimp;
@@ -159,6 +162,7 @@ namespace rlmb {
 void prof_begin(rlmb_context* ctx, const char* kernel);
 // rlmb_heevd_batched with a structure hint (band >= 0: cyclic band of that half-bandwidth).
 int heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch, int* d_info, int band);
+void tune_free(rlmb_context* ctx);
 void prof_end(rlmb_context* ctx);
 }  // namespace rlmb
 

@@ -28,6 +28,8 @@
 #include "zgemm_tc.cuh"
 
 #include <cfloat>
+#include <map>
+#include <vector>
 #include <cmath>
 
 namespace rlmb {
@@ -1983,6 +1985,15 @@ static cudaError_t launch_hetrd(const HetrdCfg& c, cudaStream_t st, int nb, type
     return cudaGetLastError();
 }
 
+// Launch choices of one eigensolve configuration that the autotuner may set (0 / -1: the
+// built-in choice for the order).
+struct HeevTune {
+    int blocked = -1;    // 1: blocked reduction (16-column panels + GEMM updates), 0: unblocked only
+    int gemm_bt = -1;    // 1: GEMM back-transformation, 0: register-resident k_ormtr (where it fits)
+    int panel_nt = 0;    // threads per panel CTA, 256 or 512
+    int xtile = 0;       // row tile of the double-precision X -= V W' update, 64 or 128
+};
+
 // Shape of one eigensolve chunk: kernel configurations and the scratch layout per matrix
 // (byte offsets, each region a multiple of 256 bytes so that every region of a chunk
 // starts aligned whatever the chunk size).
@@ -1998,18 +2009,22 @@ struct HeevPlan {
     size_t smem_orm;
     int nblk16, nblk64;
     int npanels, m_tail;  // blocked reduction: panels of HP_W columns, then k_hetrd on m_tail
+    int panel_nt, xtile;  // tuned launch choices (0: built-in)
     size_t off_d, off_e, off_tau, off_a, off_z, off_lu, off_x, off_t, off_w, off_res, off_x1, off_cl,
         off_y, off_mu, off_st, off_pv, per;
 };
 
-static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1) {
+static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1, HeevTune tune = HeevTune{}) {
     HeevPlan p{};
+    p.panel_nt = tune.panel_nt;
+    p.xtile = tune.xtile;
     p.n = n;
     p.mixed = mixed;
     p.band = band >= 0 && 32 + 2 * band <= n ? band : -1;   // the band residual needs 32 + 2o <= n
     p.refine_steps = mixed ? refine_steps : 0;
     const size_t ce = mixed ? sizeof(cplxf) : sizeof(cplx);   // working complex element
-    p.npanels = n >= HT_BLOCKED_MIN ? (n - HT_TAIL + HP_W - 1) / HP_W : 0;
+    const bool blocked = tune.blocked < 0 ? n >= HT_BLOCKED_MIN : (tune.blocked > 0 && n > HT_TAIL + HP_W);
+    p.npanels = blocked ? (n - HT_TAIL + HP_W - 1) / HP_W : 0;
     p.m_tail = n - p.npanels * HP_W;
     p.hc = mixed ? hetrd_config<float>(p.m_tail) : hetrd_config<double>(p.m_tail);
     p.smem_tri = 4 * (size_t)n * sizeof(double) + n * sizeof(int);
@@ -2027,7 +2042,8 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.smem_orm = smem;
     // register-resident k_ormtr up to order 255 (it beats the GEMM path there), the GEMM path
     // (double precision on the DMMA engine) from 256 on
-    p.small_bt = n < BT_GEMM_MIN && (n + 256 / ch - 1) / (256 / ch) <= ORM_RPT && smem <= 220 * 1024;
+    const bool reg_fits = (n + 256 / ch - 1) / (256 / ch) <= ORM_RPT && smem <= 220 * 1024;
+    p.small_bt = reg_fits && (tune.gemm_bt < 0 ? n < BT_GEMM_MIN : tune.gemm_bt == 0);
     const size_t nn = (size_t)n * n;
     auto r256 = [](size_t v) { return (v + 255) / 256 * 256; };
     size_t off = 0;
@@ -2101,6 +2117,8 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
                 return RLMB_ERR_CUDA;
             mid = nb > sms && nb <= 2 * sms && smem_of(256) <= 113 * 1024;
         }
+        if (p.panel_nt == 256 && smem_of(256) <= 113 * 1024) mid = true;
+        if (p.panel_nt == 512) mid = false;
         auto panel = mid ? k_hetrd_panel<256, R> : k_hetrd_panel<512, R>;
         const int pnt = mid ? 256 : 512;
         const size_t smem = smem_of(pnt);
@@ -2185,11 +2203,14 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
             return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
         RLMB_CHUNK_PROF("k_ormtr");
-        // X -= V W': 64-row tiles (two CTAs per SM) on the DMMA engine, 128 in single precision
-        constexpr int BMX = std::is_same<C, cplx>::value ? 64 : 128;
-        if (launch_work_gemm<C, BMX>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs}, EpSub<C>{Xw, n},
-                                 rows, n, BT_NB, nb) != cudaSuccess)
-            return RLMB_ERR_CUDA;
+        // X -= V W': 64-row tiles (two CTAs per SM) on the DMMA engine unless tuned to 128
+        // (the tcgen05 engine of the single-precision mode has its own tile)
+        const cudaError_t ex =
+            p.xtile == 128 ? launch_work_gemm<C, 128>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs},
+                                                      EpSub<C>{Xw, n}, rows, n, BT_NB, nb)
+                           : launch_work_gemm<C, 64>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs},
+                                                     EpSub<C>{Xw, n}, rows, n, BT_NB, nb);
+        if (ex != cudaSuccess) return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
     }
     return RLMB_OK;
@@ -2333,6 +2354,113 @@ int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n,
 
 using namespace rlmb;
 
+// ----------------------------------------------------------------------- autotuner
+// Per context, per (order, precision): the launch choices of HeevTune picked by timing every
+// feasible candidate -- unblocked or blocked reduction (from order 128), 256- or 512-thread
+// panels, register-resident or GEMM back-transformation, 64- or 128-row X-update tiles (double
+// precision) -- on copies of up to 2 x SMs of the call's own matrices (at most 2 GB of them),
+// each candidate run twice and timed the second time with CUDA events.  Orders 64 .. 1024
+// are tuned; others keep the built-in choices.
+struct TuneEntry {
+    HeevTune t;
+    double ms_per_matrix;
+};
+typedef std::map<std::pair<int, int>, TuneEntry> TuneCache;
+static TuneCache& tune_cache(rlmb_context* ctx) {
+    if (!ctx->tune) ctx->tune = new TuneCache();
+    return *static_cast<TuneCache*>(ctx->tune);
+}
+void rlmb::tune_free(rlmb_context* ctx) {
+    delete static_cast<TuneCache*>(ctx->tune);
+    ctx->tune = nullptr;
+}
+
+static std::vector<HeevTune> tune_candidates(int n, bool mixed) {
+    std::vector<HeevTune> out;
+    for (int blocked = 0; blocked <= 1; ++blocked) {
+        if (blocked && n < 128) continue;
+        for (int gemm = 0; gemm <= 1; ++gemm)
+            for (int nt : {256, 512}) {
+                if (!blocked && nt == 256) continue;   // no panels: one entry
+                for (int xt : {64, 128}) {
+                    if ((!gemm || mixed) && xt == 128) continue;
+                    HeevTune t;
+                    t.blocked = blocked;
+                    t.gemm_bt = gemm;
+                    t.panel_nt = blocked ? nt : 0;
+                    t.xtile = gemm && !mixed ? xt : 0;
+                    const HeevPlan p = heev_plan(n, mixed, 2, -1, t);
+                    if (!gemm && !p.small_bt) continue;   // register back-transformation does not fit
+                    out.push_back(t);
+                }
+            }
+    }
+    return out;
+}
+
+static int autotune(rlmb_context* ctx, int n, bool mixed, int refine_steps, int band, const cplx* A, int batch,
+                    HeevTune* best) {
+    int dev = 0, sms = 148;
+    RLMB_CUDA_TRY(cudaGetDevice(&dev));
+    RLMB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t nn = (size_t)n * n;
+    const size_t cap = std::min<size_t>((size_t)2 * sms, ((size_t)2 << 30) / (nn * sizeof(cplx)));
+    const int tb = (int)std::max<size_t>(1, std::min<size_t>((size_t)batch, cap));
+    const std::vector<HeevTune> cands = tune_candidates(n, mixed);
+    size_t per = 0;
+    for (const HeevTune& t : cands) per = std::max(per, heev_plan(n, mixed, refine_steps, band, t).per);
+    void* buf = nullptr;
+    const size_t work = (size_t)tb * (2 * nn * sizeof(cplx) + n * sizeof(double) + sizeof(int)) + 1024;
+    if (cudaMalloc(&buf, work) != cudaSuccess) {
+        cudaGetLastError();
+        return RLMB_ERR_ALLOC;
+    }
+    if (int rc = ensure_workspace(ctx, (size_t)tb * per)) {
+        cudaFree(buf);
+        return rc;
+    }
+    cplx* src = static_cast<cplx*>(buf);
+    cplx* wk = src + (size_t)tb * nn;
+    double* w = reinterpret_cast<double*>(wk + (size_t)tb * nn);
+    int* info = reinterpret_cast<int*>(w + (size_t)tb * n);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = RLMB_OK;
+    if (cudaMemcpyAsync(src, A, (size_t)tb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        rc = RLMB_ERR_CUDA;
+    double best_ms = 1e300;
+    long long unused = 0;
+    void* prof = ctx->prof;
+    ctx->prof = nullptr;   // tuning launches stay out of the caller's profile
+    for (size_t c = 0; c < cands.size() && rc == RLMB_OK; ++c) {
+        const HeevPlan p = heev_plan(n, mixed, refine_steps, band, cands[c]);
+        float ms = 0.f;
+        for (int rep = 0; rep < 2 && rc == RLMB_OK; ++rep) {
+            if (cudaMemcpyAsync(wk, src, (size_t)tb * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, ctx->stream) !=
+                    cudaSuccess ||
+                cudaEventRecord(e0, ctx->stream) != cudaSuccess) {
+                rc = RLMB_ERR_CUDA;
+                break;
+            }
+            rc = heev_chunk(ctx, ctx->stream, p, wk, w, info, tb, ctx->ws, &unused);
+            if (rc == RLMB_OK && (cudaEventRecord(e1, ctx->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                  cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                rc = RLMB_ERR_CUDA;
+        }
+        if (rc == RLMB_OK && ms / tb < best_ms) {
+            best_ms = ms / tb;
+            *best = cands[c];
+        }
+    }
+    ctx->prof = prof;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(buf);
+    if (rc == RLMB_OK) tune_cache(ctx)[{n, mixed ? 1 : 0}] = TuneEntry{*best, best_ms};
+    return rc;
+}
+
 // The batched eigensolve of rlmb_heevd_batched with a structure hint: band >= 0 declares every
 // matrix a cyclic band of that half-bandwidth (the rlm Hamiltonian), which the mixed mode's
 // refinement uses for its residual; band < 0 is a dense matrix.
@@ -2340,7 +2468,19 @@ int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n,
     if (!ctx || !d_a || !d_w || n <= 0 || batch < 0) return RLMB_ERR_ARG;
     if (batch == 0) return RLMB_OK;
     RLMB_CUDA_TRY(cudaSetDevice(ctx->device));
-    const HeevPlan plan = heev_plan(n, ctx->precision == RLMB_PRECISION_MIXED, ctx->refine_steps, band);
+    const bool mixed = ctx->precision == RLMB_PRECISION_MIXED;
+    HeevTune tune;
+    {
+        TuneCache& tc = tune_cache(ctx);
+        auto it = tc.find({n, mixed ? 1 : 0});
+        if (it != tc.end()) {
+            tune = it->second.t;
+        } else if (ctx->autotune && !ctx->frozen && n >= 64 && n <= 1024) {
+            if (int rc = autotune(ctx, n, mixed, ctx->refine_steps, band, reinterpret_cast<const cplx*>(d_a), batch, &tune))
+                return rc;
+        }
+    }
+    const HeevPlan plan = heev_plan(n, mixed, ctx->refine_steps, band, tune);
     const size_t per = plan.per;
     // workspace: 8 GB, or for large orders enough for two resident matrices per SM (one
     // CTA each in k_tridiag), capped at 60 % of the free memory
@@ -2373,6 +2513,47 @@ int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n,
 
 extern "C" int rlmb_heevd_batched(rlmb_context* ctx, double* d_a, double* d_w, int n, int batch, int* d_info) {
     return rlmb::heevd_batched_band(ctx, d_a, d_w, n, batch, d_info, -1);
+}
+
+extern "C" int rlmb_set_autotune(rlmb_context* ctx, int on) {
+    if (!ctx) return RLMB_ERR_ARG;
+    ctx->autotune = on ? 1 : 0;
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_heev_config(rlmb_context* ctx, int n, int precision, int* blocked, int* gemm_bt,
+                                int* panel_threads, int* x_tile, double* ms_per_matrix) {
+    if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED)) return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
+    HeevTune t;
+    double ms = 0.0;
+    if (it != tc.end()) {
+        t = it->second.t;
+        ms = it->second.ms_per_matrix;
+    }
+    const HeevPlan p = heev_plan(n, precision == RLMB_PRECISION_MIXED, 2, -1, t);
+    if (blocked) *blocked = p.npanels > 0;
+    if (gemm_bt) *gemm_bt = !p.small_bt;
+    if (panel_threads) *panel_threads = p.panel_nt;
+    if (x_tile) *x_tile = p.xtile == 128 ? 128 : 64;
+    if (ms_per_matrix) *ms_per_matrix = ms;
+    return it != tc.end() ? 1 : 0;
+}
+
+extern "C" int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int blocked, int gemm_bt,
+                                    int panel_threads, int x_tile) {
+    if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED) || blocked < -1 ||
+        blocked > 1 || gemm_bt < -1 || gemm_bt > 1 || (panel_threads != 0 && panel_threads != 256 && panel_threads != 512) ||
+        (x_tile != 0 && x_tile != 64 && x_tile != 128))
+        return RLMB_ERR_ARG;
+    HeevTune t;
+    t.blocked = blocked;
+    t.gemm_bt = gemm_bt;
+    t.panel_nt = panel_threads;
+    t.xtile = x_tile;
+    tune_cache(ctx)[{n, precision}] = TuneEntry{t, 0.0};
+    return RLMB_OK;
 }
 
 // Batched complex GEMM C = A B (column-major complex128, A m x k, B k x n, C m x n, matrices

@@ -179,6 +179,17 @@ def full_size(which):
                     "energies", "chern", "chern_raw")
             np.savez_compressed(os.path.join(HERE, f"rlm_n{n_phi}_g16_c1_s1_full.npz"),
                                 **{k: v for k, v in r.items() if k in keep})
+    if which == "hlm8":
+        # the benchmarked hlm configuration, samples 0 .. 7 (one eighth of a bench step)
+        h = hlm_reference(48, 16, 3, 0, 32, 8, 1, only=list(range(8)), keep_mesh=False)
+        np.savez_compressed(os.path.join(HERE, "hlm_48x16_q3_b0_g32_s1_samples0-7.npz"), **h)
+    if which == "rlm512x4":
+        # rlm n_phi = 512, g = 16, samples 0 .. 3 of seed 1
+        r = rlm_reference(512, 1.0, 16.0, 16, 4, 1)
+        keep = ("n_phi", "qc", "ic", "n_mesh", "n_sample", "seed", "impurity_num", "off_head",
+                "energies", "chern", "chern_raw")
+        np.savez_compressed(os.path.join(HERE, "rlm_n512_g16_c4_s1_full.npz"),
+                            **{k: v for k, v in r.items() if k in keep})
     if which == "n3000":
         # the large rlm geometry (n_phi = 3000, 48,000 impurities, g=4), sample 0 of seed 1:
         # 25 reference zheevd calls of order 3000 (tens of minutes on 8 cores)

@@ -209,3 +209,20 @@ def test_mixed_rlm_large_order(ctx):
     assert np.abs(e[0] - eref).max() <= 1e-10 * np.abs(eref).max()
     assert np.array_equal(np.rint(c[0]), np.rint(cref))
     assert np.abs(c[0] - cref).max() < 1e-8
+
+
+def test_mixed_benchmark_geometries_more_samples(ctx):
+    """The mixed mode on hlm 48x16 g=32 samples 0 .. 7 and rlm n_phi=512 samples 0 .. 3."""
+    import rlmb
+    d = golden("hlm_48x16_q3_b0_g32_s1_samples0-7.npz")
+    e, c = ctx.hlm_mesh_solve(48, 16, 3, 0, 32, rlmb.hlm_potentials(1, 768, 8))
+    for i in range(8):
+        eref, cref = d["energies"][i], d["chern"][i]
+        assert np.abs(e[i] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[i]), np.rint(cref))
+    d = golden("rlm_n512_g16_c4_s1_full.npz")
+    e, c = ctx.rlm_mesh_solve(512, 1.0, 16.0, 16, 1, 0, 4)
+    for i in range(4):
+        eref, cref = d["energies"][i], d["chern"][i]
+        assert np.abs(e[i] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[i]), np.rint(cref))

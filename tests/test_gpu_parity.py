@@ -313,6 +313,34 @@ def test_hlm_benchmark_geometry_matches_reference(ctx):
     assert [round(float(x)) for x in c.sum(axis=1)] == [round(float(x)) for x in d["chern"].sum(axis=1)]
 
 
+def test_hlm_benchmark_geometry_samples_0_to_7(ctx):
+    """hlm 48x16, q=3, band 0, g=32, seed 1: the first eight samples of a bench step, with the
+    potentials drawn by the library's own generator."""
+    import rlmb
+    d = golden("hlm_48x16_q3_b0_g32_s1_samples0-7.npz")
+    pots = rlmb.hlm_potentials(1, 768, 8)
+    assert np.array_equal(pots, d["potentials"])
+    e, c = ctx.hlm_mesh_solve(48, 16, 3, 0, 32, pots)
+    assert ctx.last_failures == 0
+    for i in range(8):
+        eref, cref = d["energies"][i], d["chern"][i]
+        assert np.abs(e[i] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[i]), np.rint(cref))
+        assert np.abs(c[i] - cref).max() < 1e-8
+
+
+def test_rlm_512_samples_0_to_3(ctx):
+    """rlm n_phi=512 (8192 impurities, g=16, seed 1): samples 0 .. 3 in one call."""
+    d = golden("rlm_n512_g16_c4_s1_full.npz")
+    e, c = ctx.rlm_mesh_solve(512, 1.0, 16.0, 16, 1, 0, 4)
+    assert ctx.last_failures == 0
+    for i in range(4):
+        eref, cref = d["energies"][i], d["chern"][i]
+        assert np.abs(e[i] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[i]), np.rint(cref))
+        assert np.abs(c[i] - cref).max() < 1e-8
+
+
 @pytest.mark.parametrize("n_phi", [64, 128, 192, 256, 384, 512])
 def test_rlm_finite_size_geometries_match_reference(ctx, n_phi):
     """rlm at the finite-size-scaling sizes (impurity concentration 16, g=16, seed 1, sample 0)."""
@@ -402,3 +430,43 @@ def test_fss_graph_matches_mesh_solve(ctx, precision):
     finally:
         ctx.precision = 0
         fg.close()
+
+
+@pytest.mark.parametrize("n", [100, 300])
+def test_heevd_every_launch_configuration(n):
+    """Each configuration the autotuner can pick gives a correct eigendecomposition."""
+    import rlmb
+    c = rlmb.Context(0)
+    try:
+        rng = np.random.default_rng(50 + n)
+        mats = [_hermitian(rng, n) for _ in range(2)]
+        for blocked in (0, 1):
+            for gemm in (0, 1):
+                for nt in (256, 512):
+                    for xt in (64, 128):
+                        c.set_heev_config(n, blocked, gemm, nt, xt)
+                        w, X = _run_heevd(c, mats)
+                        for b, M in enumerate(mats):
+                            _check_eig(M, w[b], X[b], np.linalg.eigvalsh(M))
+    finally:
+        c.close()
+
+
+def test_heevd_autotune_picks_and_caches():
+    import rlmb
+    c = rlmb.Context(0)
+    try:
+        c.set_autotune(True)
+        rng = np.random.default_rng(77)
+        for n in (160, 320):
+            assert c.heev_config(n)[0] is False
+            mats = [_hermitian(rng, n) for _ in range(3)]
+            w, X = _run_heevd(c, mats)
+            for b, M in enumerate(mats):
+                _check_eig(M, w[b], X[b], np.linalg.eigvalsh(M))
+            tuned, cfg = c.heev_config(n)
+            assert tuned and cfg["ms_per_matrix"] > 0 and cfg["x_tile"] in (64, 128)
+            w2, X2 = _run_heevd(c, mats)    # cached choice
+            assert np.abs(w2[0] - w[0]).max() <= 1e-12 * np.abs(w[0]).max()
+    finally:
+        c.close()
