@@ -419,10 +419,19 @@ int launch_hlm_vtilde(rlmb_context* ctx, const double* pot, int lx, int ly, int 
 
 // Projected H of k-point (sample, t) into column-major buf[b*N + a] = H[a][b].
 // blockIdx.y = sample * kpts + k, kpts = number of mesh k-points given in tlist.
+// Thread = row a (its Bloch indices and hhat_a held in registers); the CTA's x-slice of the
+// columns b is walked in order, so consecutive threads store consecutive entries of a
+// column (coalesced) and every per-b quantity is a warp-uniform shared-memory broadcast.
+// The sublattice offsets (kxa - kxb) mod Lx', (kya - kyb) mod ly advance by wrap-around
+// subtraction instead of integer division.  QT: the flux denominator Q as a compile-time
+// constant (hhat_a in registers), or 0 for the generic form (hhat_a re-read from shared
+// memory).
+template <int QT>
 __global__ void __launch_bounds__(256)
 k_hlm_project(const cplx* __restrict__ hb, const cplx* __restrict__ vt, const int* __restrict__ tlist,
-              int lx, int ly, int Q, int kpts, cplx* __restrict__ H) {
+              int lx, int ly, int Qr, int kpts, cplx* __restrict__ H) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int Q = QT > 0 ? QT : Qr;
     const int Lxp = lx / Q, N = Lxp * ly, ns = lx * ly;
     cplx* sh = reinterpret_cast<cplx*>(smem_raw);   // [N*Q] hhat of this k-point
     cplx* sv = sh + (size_t)N * Q;                   // [ns]  Vt of this sample
@@ -433,16 +442,42 @@ k_hlm_project(const cplx* __restrict__ hb, const cplx* __restrict__ vt, const in
     for (int i = threadIdx.x; i < ns; i += blockDim.x) sv[i] = vt[(size_t)sample * ns + i];
     __syncthreads();
     cplx* h = H + (size_t)job * N * N;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < N * N; idx += gridDim.x * blockDim.x) {
-        const int b = idx / N, a = idx % N;
-        const int kxa = a / ly, kya = a % ly, kxb = b / ly, kyb = b % ly;
-        const int dx = (kxa - kxb + Lxp) % Lxp, dy = (kya - kyb + ly) % ly;
-        cplx acc = mk(0, 0);
-        for (int q = 0; q < Q; ++q) {
-            const cplx w = cmulc(sh[a * Q + q], sh[b * Q + q]);
-            cfma(acc, w, sv[(q * Lxp + dx) * ly + dy]);
+    // columns of this CTA: [b0, b1)
+    const int per = (N + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * per, b1 = min(N, b0 + per);
+    if (b0 >= b1) return;
+    for (int a = threadIdx.x; a < N; a += blockDim.x) {
+        const int kxa = a / ly, kya = a % ly;
+        constexpr int QR = QT > 0 ? QT : 1;
+        cplx ha[QR];
+#pragma unroll
+        for (int q = 0; q < QR; ++q) ha[q] = cconj(sh[a * Q + q]);
+        const int kxb = b0 / ly, kyb0 = b0 % ly;
+        int kyb = kyb0;
+        int dx = kxa - kxb;
+        if (dx < 0) dx += Lxp;
+        int dy = kya - kyb;
+        if (dy < 0) dy += ly;
+        for (int b = b0; b < b1; ++b) {
+            cplx acc = mk(0, 0);
+            const cplx* hbq = sh + b * Q;
+            if constexpr (QT > 0) {
+#pragma unroll
+                for (int q = 0; q < QT; ++q) cfma(acc, cmul(ha[q], hbq[q]), sv[(q * Lxp + dx) * ly + dy]);
+            } else {
+                for (int q = 0; q < Q; ++q)
+                    cfma(acc, cmul(cconj(sh[a * Q + q]), hbq[q]), sv[(q * Lxp + dx) * ly + dy]);
+            }
+            h[(size_t)b * N + a] = acc;
+            // next column: kyb + 1 (wrapping into kxb + 1)
+            if (++kyb == ly) {
+                kyb = 0;
+                dy = kya;
+                if (--dx < 0) dx += Lxp;
+            } else if (--dy < 0) {
+                dy += ly;
+            }
         }
-        h[idx] = acc;
     }
 }
 
@@ -451,11 +486,13 @@ int launch_hlm_project(rlmb_context* ctx, const cplx* hb, const cplx* vt, const 
     const int N = lx * ly / Q;
     const size_t smem = ((size_t)N * Q + (size_t)lx * ly) * sizeof(cplx);
     if (smem > 200 * 1024) return RLMB_ERR_ARG;
-    RLMB_CUDA_TRY(cudaFuncSetAttribute(k_hlm_project, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int bx = std::max(1, std::min((N * N + 255) / 256, 64));
+    auto kern = Q == 1 ? k_hlm_project<1> : Q == 2 ? k_hlm_project<2> : Q == 3 ? k_hlm_project<3>
+              : Q == 4 ? k_hlm_project<4> : k_hlm_project<0>;
+    RLMB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int bx = std::max(1, std::min(N / 32, 16));   // column slices of >= 32 columns per k-point
     dim3 grid(bx, kpts * nsamples);
     prof_begin(ctx, "k_hlm_project");
-    k_hlm_project<<<grid, 256, smem, ctx->stream>>>(hb, vt, d_tlist, lx, ly, Q, kpts, H);
+    kern<<<grid, 256, smem, ctx->stream>>>(hb, vt, d_tlist, lx, ly, Q, kpts, H);
     RLMB_LAUNCHED(ctx);
     return RLMB_OK;
 }
