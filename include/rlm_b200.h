@@ -122,9 +122,14 @@ int rlmb_heevd_batched_noalloc(double* d_a, double* d_w, int n, int batch, int* 
  * engine RLMB_GEMM_FP64: double precision on the FP64 tensor path (DMMA);
  * engine RLMB_GEMM_TF32X3: the tcgen05 tensor cores, each operand split into two TF32
  * numbers and three products accumulated in FP32 (relative error ~1e-6 of |A||B|), the
- * engine of the mixed-precision eigensolver's products.  batch <= 65535. */
+ * engine of the reduction's and back-transformation's products in the mixed mode;
+ * engine RLMB_GEMM_TF32X3_F64ACC: the same products with the operands loaded by TMA from
+ * TF32 planes and the accumulator emptied into double-precision sums after every 32 real
+ * terms (relative error ~1e-7 of |A||B|), the engine of the mixed mode's refinement products.
+ * batch <= 65535; with k = 0 the product is zero and d_a, d_b may be NULL. */
 #define RLMB_GEMM_FP64 0
 #define RLMB_GEMM_TF32X3 1
+#define RLMB_GEMM_TF32X3_F64ACC 2
 int rlmb_zgemm_batched(rlmb_context* ctx, const double* d_a, const double* d_b, double* d_c, int m, int n,
                        int k, int batch, int engine);
 /* Tiles of the tcgen05 engine whose bounded mbarrier waits ran out (a fault: the tile's

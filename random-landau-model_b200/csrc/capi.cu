@@ -33,6 +33,7 @@ static int grow(rlmb_context* ctx, void** buf, size_t* have, size_t bytes) {
 int ensure_workspace(rlmb_context* ctx, size_t bytes) { return grow(ctx, &ctx->ws, &ctx->ws_bytes, bytes); }
 int ensure_pipe(rlmb_context* ctx, size_t bytes) { return grow(ctx, &ctx->pipe, &ctx->pipe_bytes, bytes); }
 static int ensure_io(rlmb_context* ctx, size_t bytes) { return grow(ctx, &ctx->io, &ctx->io_bytes, bytes); }
+int ensure_tma_planes(rlmb_context* ctx, size_t bytes) { return grow(ctx, &ctx->tws, &ctx->tws_bytes, bytes); }
 int ensure_pinned(rlmb_context* ctx, size_t bytes) {
     if (bytes <= ctx->pinned_bytes) return RLMB_OK;
     if (ctx->pinned) {
@@ -192,6 +193,7 @@ int rlmb_destroy(rlmb_context* ctx) {
     if (ctx->ws) cudaFree(ctx->ws);
     if (ctx->pipe) cudaFree(ctx->pipe);
     if (ctx->io) cudaFree(ctx->io);
+    if (ctx->tws) cudaFree(ctx->tws);
     if (ctx->fail) cudaFree(ctx->fail);
     if (ctx->mt_state) cudaFree(ctx->mt_state);
     if (ctx->hlm_tables) cudaFree(ctx->hlm_tables);

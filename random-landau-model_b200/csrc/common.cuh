@@ -127,6 +127,9 @@ struct rlmb_context {
     uint32_t* mt_state;
     // set while a stream capture records this context's work: buffers may not grow then
     int frozen;
+    // TF32 operand planes of the TMA-fed tensor-core GEMMs (grow-only)
+    void* tws;
+    size_t tws_bytes;
     // eigensolver autotuning (rlmb_set_autotune) and its per-(order, precision) choices
     int autotune;
     void* tune;
@@ -182,6 +185,7 @@ namespace rlmb {
 // Grow-only workspace of the context (cudaMallocAsync on its stream would also do; a
 // plain grow-only buffer keeps repeated calls allocation-free).
 int ensure_workspace(rlmb_context* ctx, size_t bytes);
+int ensure_tma_planes(rlmb_context* ctx, size_t bytes);
 int ensure_pipe(rlmb_context* ctx, size_t bytes);
 int ensure_pinned(rlmb_context* ctx, size_t bytes);
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }

@@ -26,6 +26,7 @@
 #include "small_eig.cuh"
 #include "zgemm.cuh"
 #include "zgemm_tc.cuh"
+#include "zgemm_tma.cuh"
 
 #include <cfloat>
 #include <map>
@@ -1300,10 +1301,15 @@ static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked re
 // contributions conj(A[r][c]) v[r] stay in registers for the whole strip and are reduced
 // across the warp once at the end.  Interior blocks (entirely above the diagonal and inside
 // the matrix) run without predicates.
-static constexpr int HV_W = 8;
+// Strip width: 8 columns in double precision, 16 in single precision, so that a lane has the
+// same bytes of loads in flight (128) in both modes: the product streams the leading block
+// from memory and is bound by the loads each SM keeps in flight, not by its arithmetic.
+template <class C>
+__host__ __device__ constexpr int hv_width() { return sizeof(C) == 8 ? 16 : 8; }
 template <int NT, class C>
 __device__ __forceinline__ void hemv_upper(const C* __restrict__ a, int ld, int m, const C* __restrict__ v,
                                            C* p) {
+    constexpr int HV_W = hv_width<C>();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = NT / 32;
     const int nstrips = (m + HV_W - 1) / HV_W;
@@ -2010,6 +2016,10 @@ struct HeevPlan {
     int nblk16, nblk64;
     int npanels, m_tail;  // blocked reduction: panels of HP_W columns, then k_hetrd on m_tail
     int panel_nt, xtile;  // tuned launch choices (0: built-in)
+    // per: bytes per matrix of the chunk's regions (offsets off_*, times the chunk size);
+    // per2: bytes per matrix of the mixed mode's refinement regions (Res, X1), which the
+    // refinement uses for one sub-chunk of matrices at a time
+    size_t per2, off2_x1;
     size_t off_d, off_e, off_tau, off_a, off_z, off_lu, off_x, off_t, off_w, off_res, off_x1, off_cl,
         off_y, off_mu, off_st, off_pv, per;
 };
@@ -2056,14 +2066,17 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.off_x = off; off += r256(nn * ce);
     p.off_t = off; off += r256((p.small_bt ? (size_t)p.nblk16 * ORM_NB * ORM_NB : (size_t)p.nblk64 * BT_NB * BT_NB) * ce);
     p.off_w = off; off += p.small_bt ? 0 : r256(2 * (size_t)BT_NB * n * ce);   // G and W' of a block
-    p.off_res = off; off += mixed ? r256(nn * sizeof(cplx)) : 0;
-    p.off_x1 = off; off += p.refine_steps >= 2 ? r256(nn * sizeof(cplx)) : 0;   // step-1 vectors
+    p.off_res = 0;   // (the refinement regions: per2 below)
+    p.off_x1 = 0;
     p.off_cl = off; off += mixed ? r256(n * sizeof(int2)) : 0;
     p.off_y = off; off += mixed ? r256((size_t)n * RF_KMAX * sizeof(cplx)) : 0;
     p.off_mu = off; off += mixed ? r256(n * sizeof(double)) : 0;
     p.off_st = off; off += mixed ? r256(3 * (size_t)n * sizeof(double)) : 0;
     p.off_pv = off; off += p.npanels > 0 ? r256(2 * (size_t)HP_W * n * ce) : 0;   // panel V, W
     p.per = off;
+    p.per2 = mixed ? r256(nn * sizeof(cplx)) : 0;                              // residual R
+    p.off2_x1 = p.per2;
+    p.per2 += p.refine_steps >= 2 ? r256(nn * sizeof(cplx)) : 0;                 // step-1 vectors
     return p;
 }
 
@@ -2216,6 +2229,30 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
     return RLMB_OK;
 }
 
+// cuTensorMapEncodeTiled, looked up once from the driver through the runtime.
+TmaEncodeFn tma_encode_fn() {
+    static TmaEncodeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<TmaEncodeFn>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Planes of the TMA-fed GEMMs of one refinement chunk: up to 4 GB, at least one matrix.
+static int refine_planes(rlmb_context* ctx, int n, int nb) {
+    const size_t per = tma_plane_bytes(n, n, n);
+    const size_t want = std::max(per, std::min((size_t)nb * per, (size_t)4 << 30));
+    return ensure_tma_planes(ctx, want);
+}
+
 // One refinement step from the vectors X (single or double) to Out (double, not X).
 template <class XT>
 static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int nb, const cplx* A, const XT* X,
@@ -2238,8 +2275,13 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int 
     k_ref_clusters<<<(nb + 127) / 128, 128, 0, st>>>(W, ST, CL, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_coupling");
-    if (launch_zgemm_tc<cplx>(st, OpRowA<cplx, XT, true>{X, n, nn}, OpColB<cplx, cplx>{Res, n, nn},
-                                EpCoupling<XT>{X, W, CL, F, n}, n, n, n, nb) != cudaSuccess)
+    // E = X^H R on the TMA-fed engine with double-precision accumulation: its error, relative
+    // to |X| |R|, is the orthogonality defect the step leaves (F + F^H cancels x_i^H x_j only
+    // as well as E is known)
+    if (!ctx) return RLMB_ERR_ARG;
+    if (int rc = refine_planes(ctx, n, nb)) return rc;
+    if (launch_zgemm_tma<cplx>(st, OpRowA<cplx, XT, true>{X, n, nn}, OpColB<cplx, cplx>{Res, n, nn},
+                               EpCoupling<XT>{X, W, CL, F, n}, n, n, n, nb, ctx->tws, ctx->tws_bytes) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_cluster");
@@ -2257,8 +2299,8 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int 
     k_ref_diag<<<(unsigned)(((size_t)nb * n + 255) / 256), 256, 0, st>>>(ST, CL, W, F, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_update");
-    if (launch_zgemm_tc<cplxf>(st, OpColA<cplx, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
-                                 EpUpdate<XT>{X, Out, n}, n, n, n, nb) != cudaSuccess)
+    if (launch_zgemm_tma<cplxf>(st, OpColA<cplx, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
+                                EpUpdate<XT>{X, Out, n}, n, n, n, nb, ctx->tws, ctx->tws_bytes) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_cluster");
@@ -2272,7 +2314,7 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int 
 // region is written by a kernel before any kernel reads it.  ctx (optional) receives the
 // launch count and profile; otherwise *launches is advanced.
 static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cplx* A, double* W, int* info,
-                      int nb, void* scratch, long long* launches) {
+                      int nb, void* scratch, int nb2, long long* launches) {
     const int n = p.n;
     unsigned char* base = static_cast<unsigned char*>(scratch);
     const size_t B = (size_t)nb;
@@ -2309,8 +2351,10 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     cplxf* Xw = reinterpret_cast<cplxf*>(base + p.off_x * B);
     cplxf* Tw = reinterpret_cast<cplxf*>(base + p.off_t * B);
     cplxf* Wp = reinterpret_cast<cplxf*>(base + p.off_w * B);
-    cplx* Res = reinterpret_cast<cplx*>(base + p.off_res * B);
-    cplx* X1 = reinterpret_cast<cplx*>(base + p.off_x1 * B);
+    // refinement regions for nb2 matrices at a time, after the chunk's regions
+    unsigned char* base2 = base + p.per * B;
+    cplx* Res = reinterpret_cast<cplx*>(base2);
+    cplx* X1 = reinterpret_cast<cplx*>(base2 + p.off2_x1 * (size_t)nb2);
     int2* CL = reinterpret_cast<int2*>(base + p.off_cl * B);
     cplx* YB = reinterpret_cast<cplx*>(base + p.off_y * B);
     double* MU = reinterpret_cast<double*>(base + p.off_mu * B);
@@ -2331,15 +2375,29 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
     RLMB_CHUNK_LAUNCHED();
     if (int rc = back_transform<float>(ctx, st, p, nb, As, TAUw, Zw, Xw, Tw, Wp, launches)) return rc;
-    // refinement: the single-precision copy of H is free now and holds F.  Step 1 starts
-    // from the single-precision vectors, step 2 from step 1's double vectors (X1); the
-    // last step writes the caller's buffer (every step's residual reads H first).
-    if (int rc = refine_step<cplxf>(ctx, st, n, p.band, nb, A, Xw, W, Res, As, CL, YB, MU, ST,
-                                    p.refine_steps >= 2 ? X1 : A, launches))
-        return rc;
-    if (p.refine_steps >= 2)
-        if (int rc = refine_step<cplx>(ctx, st, n, p.band, nb, A, X1, W, Res, As, CL, YB, MU, ST, A, launches))
+    // refinement, nb2 matrices at a time: the single-precision copy of H is free now and
+    // holds F.  Step 1 starts from the single-precision vectors, step 2 from step 1's double
+    // vectors (X1); the last step writes the caller's buffer (every step's residual reads H
+    // first).
+    if (nb2 < 1) return RLMB_ERR_ARG;
+    for (int m0 = 0; m0 < nb; m0 += nb2) {
+        const int ns = std::min(nb2, nb - m0);
+        const size_t o = (size_t)m0 * nn, on = (size_t)m0 * n;
+        cplx* Am = A + o;
+        double* Wm = W + on;
+        cplxf* Fm = As + o;
+        int2* CLm = CL + on;
+        cplx* YBm = YB + (size_t)m0 * n * RF_KMAX;
+        double* MUm = MU + on;
+        double* STm = ST + 3 * on;
+        if (int rc = refine_step<cplxf>(ctx, st, n, p.band, ns, Am, Xw + o, Wm, Res, Fm, CLm, YBm, MUm, STm,
+                                        p.refine_steps >= 2 ? X1 : Am, launches))
             return rc;
+        if (p.refine_steps >= 2)
+            if (int rc = refine_step<cplx>(ctx, st, n, p.band, ns, Am, X1, Wm, Res, Fm, CLm, YBm, MUm, STm, Am,
+                                           launches))
+                return rc;
+    }
     return RLMB_OK;
 }
 #undef RLMB_CHUNK_LAUNCHED
@@ -2347,7 +2405,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
 
 int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n, int nb, void* scratch,
                           long long* launches) {
-    return heev_chunk(nullptr, st, heev_plan(n, false), A, W, info, nb, scratch, launches);
+    return heev_chunk(nullptr, st, heev_plan(n, false), A, W, info, nb, scratch, 0, launches);
 }
 
 }  // namespace rlmb
@@ -2408,7 +2466,10 @@ static int autotune(rlmb_context* ctx, int n, bool mixed, int refine_steps, int 
     const int tb = (int)std::max<size_t>(1, std::min<size_t>((size_t)batch, cap));
     const std::vector<HeevTune> cands = tune_candidates(n, mixed);
     size_t per = 0;
-    for (const HeevTune& t : cands) per = std::max(per, heev_plan(n, mixed, refine_steps, band, t).per);
+    for (const HeevTune& t : cands) {
+        const HeevPlan pl = heev_plan(n, mixed, refine_steps, band, t);
+        per = std::max(per, pl.per + pl.per2);
+    }
     void* buf = nullptr;
     const size_t work = (size_t)tb * (2 * nn * sizeof(cplx) + n * sizeof(double) + sizeof(int)) + 1024;
     if (cudaMalloc(&buf, work) != cudaSuccess) {
@@ -2442,7 +2503,7 @@ static int autotune(rlmb_context* ctx, int n, bool mixed, int refine_steps, int 
                 rc = RLMB_ERR_CUDA;
                 break;
             }
-            rc = heev_chunk(ctx, ctx->stream, p, wk, w, info, tb, ctx->ws, &unused);
+            rc = heev_chunk(ctx, ctx->stream, p, wk, w, info, tb, ctx->ws, tb, &unused);
             if (rc == RLMB_OK && (cudaEventRecord(e1, ctx->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
                                   cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
                 rc = RLMB_ERR_CUDA;
@@ -2489,23 +2550,33 @@ int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n,
         cudaGetLastError();
         free_b = (size_t)8 << 30;
     }
-    size_t budget = std::max<size_t>((size_t)8 << 30, 2 * 148 * per);
+    const size_t per2 = plan.per2;
+    size_t budget = std::max<size_t>((size_t)8 << 30, 2 * 148 * (per + per2));
     budget = std::min<size_t>(budget, free_b / 10 * 6 + ctx->ws_bytes);
-    budget = std::max<size_t>(budget, per);
-    if (ctx->frozen) budget = std::max<size_t>(per, ctx->ws_bytes);   // capture: the workspace as sized before
-    size_t chunk = std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)batch));
+    budget = std::max<size_t>(budget, per + per2);
+    if (ctx->frozen) budget = std::max<size_t>(per + per2, ctx->ws_bytes);   // capture: the workspace as sized before
+    // the refinement regions take up to an eighth of the budget (its GEMMs fill the GPU from a
+    // few matrices on); the chunk -- all of whose matrices the one-CTA-per-matrix reduction and
+    // tridiagonal kernels run at once -- takes the rest
+    size_t nb2 = per2 ? std::max<size_t>(1, std::min<size_t>((size_t)batch, budget / 8 / per2)) : 0;
+    size_t chunk = std::max<size_t>(1, std::min<size_t>((budget - nb2 * per2) / per, (size_t)batch));
     chunk = std::min<size_t>(chunk, 65535);   // grid y / z extent of the per-matrix launches
     if (!plan.small_bt) chunk = std::min<size_t>(chunk, 65535 / std::max(plan.nblk64, 1));   // (matrix, block) batches
     // equal chunks: a short last chunk would leave most SMs idle in the one-CTA-per-matrix kernels
     const size_t nchunks = (batch + chunk - 1) / chunk;
     chunk = (batch + nchunks - 1) / nchunks;
-    if (int rc = ensure_workspace(ctx, chunk * per)) return rc;
+    if (per2) {   // equal refinement sub-chunks too
+        nb2 = std::min(nb2, chunk);
+        const size_t nsub = (chunk + nb2 - 1) / nb2;
+        nb2 = (chunk + nsub - 1) / nsub;
+    }
+    if (int rc = ensure_workspace(ctx, chunk * per + nb2 * per2)) return rc;
     const size_t nn = (size_t)n * n;
     long long unused = 0;
     for (size_t b0 = 0; b0 < (size_t)batch; b0 += chunk) {
         const int nb = (int)std::min(chunk, (size_t)batch - b0);
         if (int rc = heev_chunk(ctx, ctx->stream, plan, reinterpret_cast<cplx*>(d_a) + b0 * nn, d_w + b0 * n,
-                                d_info ? d_info + b0 : nullptr, nb, ctx->ws, &unused))
+                                d_info ? d_info + b0 : nullptr, nb, ctx->ws, (int)nb2, &unused))
             return rc;
     }
     return RLMB_OK;
@@ -2561,8 +2632,8 @@ extern "C" int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int
 // tensor cores with split operands (FP32-class accuracy).
 extern "C" int rlmb_zgemm_batched(rlmb_context* ctx, const double* d_a, const double* d_b, double* d_c, int m,
                                   int n, int k, int batch, int engine) {
-    if (!ctx || !d_a || !d_b || !d_c || m <= 0 || n <= 0 || k < 0 || batch < 0 ||
-        (engine != RLMB_GEMM_FP64 && engine != RLMB_GEMM_TF32X3))
+    if (!ctx || (k > 0 && (!d_a || !d_b)) || !d_c || m <= 0 || n <= 0 || k < 0 || batch < 0 ||
+        (engine != RLMB_GEMM_FP64 && engine != RLMB_GEMM_TF32X3 && engine != RLMB_GEMM_TF32X3_F64ACC))
         return RLMB_ERR_ARG;
     if (batch == 0) return RLMB_OK;
     if (batch > 65535) return RLMB_ERR_ARG;
@@ -2573,9 +2644,15 @@ extern "C" int rlmb_zgemm_batched(rlmb_context* ctx, const double* d_a, const do
     const OpColA<cplx, cplx> la{A, m, (size_t)m * k};
     const OpColB<cplx, cplx> lb{B, k, (size_t)k * n};
     const EpStore<cplx> ep{Cm, m, (size_t)m * n};
-    prof_begin(ctx, engine == RLMB_GEMM_FP64 ? "k_zgemm_dmma" : "k_zgemm_tc");
-    const cudaError_t e = engine == RLMB_GEMM_FP64 ? launch_zgemm<cplx, 64>(ctx->stream, la, lb, ep, m, n, k, batch)
-                                                   : launch_zgemm_tc<cplx>(ctx->stream, la, lb, ep, m, n, k, batch);
+    if (engine == RLMB_GEMM_TF32X3_F64ACC && k > 0) {
+        const size_t per = tma_plane_bytes(m, n, k);
+        if (int rc = ensure_tma_planes(ctx, std::max(per, std::min((size_t)batch * per, (size_t)4 << 30)))) return rc;
+    }
+    prof_begin(ctx, engine == RLMB_GEMM_FP64 ? "k_zgemm_dmma" : engine == RLMB_GEMM_TF32X3 ? "k_zgemm_tc" : "k_zgemm_tma");
+    const cudaError_t e =
+        engine == RLMB_GEMM_FP64     ? launch_zgemm<cplx, 64>(ctx->stream, la, lb, ep, m, n, k, batch)
+        : engine == RLMB_GEMM_TF32X3 ? launch_zgemm_tc<cplx>(ctx->stream, la, lb, ep, m, n, k, batch)
+                                     : launch_zgemm_tma<cplx>(ctx->stream, la, lb, ep, m, n, k, batch, ctx->tws, ctx->tws_bytes);
     prof_end(ctx);
     ctx->launches++;
     return e == cudaSuccess ? RLMB_OK : RLMB_ERR_CUDA;

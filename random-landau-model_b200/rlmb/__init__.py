@@ -270,7 +270,7 @@ class Context:
         _check(lib().rlmb_set_heev_config(self.h, n, prec, blocked, gemm_bt, panel_threads, x_tile),
                "rlmb_set_heev_config")
 
-    GEMM_FP64, GEMM_TF32X3 = 0, 1
+    GEMM_FP64, GEMM_TF32X3, GEMM_TF32X3_F64ACC = 0, 1, 2
 
     def zgemm(self, at, bt, engine=GEMM_TF32X3):
         """C = A B for torch complex128 CUDA tensors at[batch, k, m] = A^T and bt[batch, n, k] =
