@@ -2138,11 +2138,11 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         if (cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return RLMB_ERR_CUDA;
         for (int k = 0; k < p.npanels; ++k) {
-            RLMB_CHUNK_PROF("k_hetrd");
+            RLMB_CHUNK_PROF("k_hetrd_panel");
             panel<<<nb, pnt, smem, st>>>(A, D, E, TAU, PV, PWb, n, m);
             RLMB_CHUNK_LAUNCHED();
             m -= HP_W;
-            RLMB_CHUNK_PROF("k_hetrd");
+            RLMB_CHUNK_PROF("k_hetrd_her2k");
             if (launch_work_gemm<C, 64>(st, OpPanelA<C>{PV, PWb, n}, OpPanelB<C>{PV, PWb, n}, EpHer2k<C>{A, n}, m, m,
                                     2 * HP_W, nb) != cudaSuccess)
                 return RLMB_ERR_CUDA;
