@@ -1270,7 +1270,8 @@ struct EpSub {     // X(r, c) -= acc
         C* q = x + mat * (size_t)n * n + (size_t)c * n + r;
         *q = csub(*q, acc);
     }
-    // the DMMA engine prefetches X(r, c) into shared memory and passes it back as `old`
+    // the GEMM engines prefetch X(r, c) (the DMMA engine into shared memory, the tcgen05
+    // engine into registers) and pass it back as `old`
     __device__ __forceinline__ const C* pre_src(size_t mat, int r, int c) const {
         return x + mat * (size_t)n * n + (size_t)c * n + r;
     }
@@ -1511,7 +1512,7 @@ struct EpHer2k {
         if (r == c) x.y = 0;
         *q = x;
     }
-    // the DMMA engine prefetches A(r, c) (on and above the diagonal) into shared memory
+    // the GEMM engines prefetch A(r, c) (on and above the diagonal) when the tile starts
     __device__ __forceinline__ const C* pre_src(size_t mat, int r, int c) const {
         return r > c ? nullptr : a + mat * (size_t)n * n + (size_t)c * n + r;
     }

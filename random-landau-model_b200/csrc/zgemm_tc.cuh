@@ -16,7 +16,8 @@
 // product term plus the FP32 accumulation.  TF32 products of 11-bit operands are exact in
 // FP32.
 //
-// Pipeline (one CTA of 256 threads per output tile, one CTA per SM by shared memory):
+// Pipeline (one CTA of 256 threads per output tile; three stages and one CTA per SM, or for
+// short inner dimensions one stage and two CTAs per SM):
 //   * all threads load the next K block (16 complex k) of A and B through the accessors into
 //     registers one block ahead, split it and store it to a free stage of shared memory in
 //     the canonical K-major 128-byte-swizzled layout (8-row atoms of 128-byte rows, the
@@ -35,6 +36,7 @@
 #include "common.cuh"
 
 #include <type_traits>
+#include <utility>
 
 namespace rlmb {
 
@@ -141,11 +143,32 @@ struct tc_has_skip : std::false_type {};
 template <class T>
 struct tc_has_skip<T, std::void_t<decltype(&T::skip_tile)>> : std::true_type {};
 
-template <class C, class LA, class LB, class EP>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+// An epilogue that updates C in place may expose pre_src(mat, r, c) (address of C(r, c), or
+// null where it writes nothing) and store_pre(mat, r, c, acc, old): each thread then loads
+// its 32 entries of C into registers when the tile starts, so that these reads overlap the
+// operand loads and the MMAs instead of following them.
+template <class T, class = void>
+struct tc_has_pre : std::false_type {};
+template <class T>
+struct tc_has_pre<T, std::void_t<decltype(&T::pre_src)>> : std::true_type {};
+template <class EP, bool P = tc_has_pre<EP>::value>
+struct tc_pre_type {
+    typedef float2 T;
+};
+template <class EP>
+struct tc_pre_type<EP, true> {
+    typedef std::remove_cv_t<std::remove_pointer_t<decltype(std::declval<EP>().pre_src(0, 0, 0))>> T;
+};
+
+// STAGES shared-memory stages of one K block each; MINB CTAs per SM.  Short inner
+// dimensions (K <= 4 blocks: the rank-32 panel updates, the 64-reflector block updates)
+// take one stage and two CTAs per SM, so that one CTA's epilogue overlaps the other's
+// loads; the next block's global loads are in flight while the tensor core reads the stage.
+template <class C, class LA, class LB, class EP, int STAGES = TC_STAGES, int MINB = 1>
+__global__ void __launch_bounds__(TC_THREADS, MINB)
 k_zgemm_tc(LA la, LB lb, EP ep, int M, int N, int K) {
     extern __shared__ unsigned char tc_raw[];
-    __shared__ __align__(8) uint64_t bar_free[TC_STAGES];
+    __shared__ __align__(8) uint64_t bar_free[STAGES];
     __shared__ __align__(8) uint64_t bar_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int fault;
@@ -166,6 +189,24 @@ k_zgemm_tc(LA la, LB lb, EP ep, int M, int N, int K) {
     if (skip_cta) return;
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~(uintptr_t)1023);
     const uint32_t sbase = tc_smem_u32(smem);
+    // epilogue coordinates of this thread: TMEM lane quarter q, accumulator columns cbase..+63,
+    // row r; entry i = 8 (chunk of 16 columns) + j sits at column c0 + cbase + 16 (i / 8) +
+    // (i % 8) + (odd ? 8 : 0)
+    const int q = warp & 3;
+    const int cbase = (warp >> 2) * 64;
+    const bool odd = lane & 1;   // odd lanes hold imaginary parts
+    const int r = r0 + 16 * q + (lane >> 1);
+    constexpr bool PRE = tc_has_pre<EP>::value;
+    typedef typename tc_pre_type<EP>::T CO;
+    CO old[PRE ? 32 : 1];
+    if constexpr (PRE) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            const int c = c0 + cbase + 16 * (i >> 3) + (i & 7) + (odd ? 8 : 0);
+            const CO* src = (r < M && c < N) ? ep.pre_src(mat, r, c) : nullptr;
+            old[i] = src ? *src : CO{};
+        }
+    }
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_u32(&tmem_slot)),
@@ -174,7 +215,7 @@ k_zgemm_tc(LA la, LB lb, EP ep, int M, int N, int K) {
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (t == 32) {
-        for (int s = 0; s < TC_STAGES; ++s) tc_mbar_init(&bar_free[s], 1);
+        for (int s = 0; s < STAGES; ++s) tc_mbar_init(&bar_free[s], 1);
         tc_mbar_init(&bar_done, 1);
         fault = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -246,10 +287,10 @@ k_zgemm_tc(LA la, LB lb, EP ep, int M, int N, int K) {
     int issued = 0;   // thread 0: whether any MMA was issued
     if (nk > 0) load(0);
     for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % TC_STAGES;
-        if (kb >= TC_STAGES) {
-            // the stage is free once the MMAs of block kb - TC_STAGES have read it
-            if (!tc_mbar_wait(&bar_free[s], (unsigned)((kb / TC_STAGES - 1) & 1))) atomicExch(&fault, 1);
+        const int s = kb % STAGES;
+        if (kb >= STAGES) {
+            // the stage is free once the MMAs of block kb - STAGES have read it
+            if (!tc_mbar_wait(&bar_free[s], (unsigned)((kb / STAGES - 1) & 1))) atomicExch(&fault, 1);
         }
         __syncthreads();
         if (fault) break;
@@ -281,11 +322,7 @@ k_zgemm_tc(LA la, LB lb, EP ep, int M, int N, int K) {
     tc_fence_after();
     __syncthreads();
     if (!fault) {
-        const int q = warp & 3;             // TMEM lane quarter of this warp
-        const int cbase = (warp >> 2) * 64; // accumulator columns of this warp
-        const bool odd = lane & 1;          // odd lanes hold imaginary parts
-        const int r = r0 + 16 * q + (lane >> 1);
-#pragma unroll 1
+#pragma unroll
         for (int ch = 0; ch < 64; ch += 16) {
             float v[16];
             if (any_issued) {
@@ -299,7 +336,14 @@ k_zgemm_tc(LA la, LB lb, EP ep, int M, int N, int K) {
             for (int j = 0; j < 8; ++j) {
                 const float x = __shfl_xor_sync(0xffffffffu, odd ? v[j] : v[j + 8], 1);
                 const int c = c0 + cbase + ch + j + (odd ? 8 : 0);
-                if (r < M && c < N) ep.store(mat, r, c, cm<C>(odd ? x : v[j], odd ? v[j + 8] : x));
+                if (r < M && c < N) {
+                    const C acc = cm<C>(odd ? x : v[j], odd ? v[j + 8] : x);
+                    if constexpr (PRE) {
+                        if (ep.pre_src(mat, r, c)) ep.store_pre(mat, r, c, acc, old[(ch >> 4) * 8 + j]);
+                    } else {
+                        ep.store(mat, r, c, acc);
+                    }
+                }
             }
         }
     } else if (t == 0) {
@@ -318,10 +362,12 @@ cudaError_t launch_zgemm_tc(cudaStream_t st, const LA& la, const LB& lb, const E
     if (M <= 0 || N <= 0 || nb <= 0) return cudaSuccess;
     const dim3 grid((M + TC_BM - 1) / TC_BM, (N + TC_BN - 1) / TC_BN, nb);
     if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
-    auto kern = k_zgemm_tc<C, LA, LB, EP>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+    const bool short_k = K <= 4 * TC_KB;
+    auto kern = short_k ? k_zgemm_tc<C, LA, LB, EP, 1, 2> : k_zgemm_tc<C, LA, LB, EP, TC_STAGES, 1>;
+    const size_t smem = short_k ? (size_t)TC_STAGE + 1024 : TC_SMEM;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, TC_THREADS, TC_SMEM, st>>>(la, lb, ep, M, N, K);
+    kern<<<grid, TC_THREADS, smem, st>>>(la, lb, ep, M, N, K);
     return cudaGetLastError();
 }
 
