@@ -337,6 +337,15 @@ def _with_reduction(prof):
     return out
 
 
+# algorithmic DRAM bytes per matrix of the blocked reduction's panels at order n (FP64): the
+# stored triangle of the leading c x c block read once for every column c the panels reduce
+# (columns n-1 down to the unblocked tail's order; panels of 16 columns, tail order < 64 + 16)
+def _panel_bytes_per_matrix(n, width=16, tail=64, elem=16):
+    npanels = (n - tail + width - 1) // width if n >= 256 else 0
+    m_tail = n - npanels * width
+    return elem * sum(c * (c + 1) / 2 for c in range(m_tail, n))
+
+
 # algorithmic FP64 flops per matrix of n_phi (LAPACK counts: zhetrd 16/3 n^3, zunmtr 8 n^3)
 def _kernel_flops_per_matrix(kernel, n):
     return {"reduction": 16.0 / 3.0 * n ** 3, "k_ormtr": 8.0 * n ** 3}.get(kernel)
@@ -733,23 +742,34 @@ def run_headline(args):
                 par[mode] = {"max_energy_rel_error": float(np.abs(e[0] - eref).max() / np.abs(eref).max()),
                              "chern_integers_identical": bool(np.array_equal(np.rint(c[0]), np.rint(cref))),
                              "max_chern_deviation": float(np.abs(c[0] - cref).max())}
-        # dominant kernel label of the FP64 step and its FP64 roofline (algorithmic flops)
         total_ms = sum(v[0] for v in prof.values())
-        prof_r = {k: v for k, v in _with_reduction(prof).items() if k not in REDUCTION_LABELS}
-        kname, (kms, klaunch) = max(prof_r.items(), key=lambda kv: kv[1][0])
-        fpm = _kernel_flops_per_matrix(kname, n)
+        # the dominant kernel of the FP64 step, k_hetrd_panel, is bound by HBM: each column's
+        # Hermitian matrix-vector product streams the stored triangle of the leading block
         roof = None
-        if fpm is not None:
-            achieved = fpm * solves * args.steps / (kms * 1e-3) / 1e12
-            tr = _traffic_per_matrix(kname, n)
-            roof = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp64_peak, "traffic": tr * solves * args.steps / klaunch if tr else None,
-                    "peak_source": "measured in this run: FP64 FMA throughput probe (MEASURED_PEAKS.json holds "
-                                   "no FP64 figure)",
-                    "share_of_gpu_time": kms / total_ms, "launches": klaunch,
-                    "note": "achieved = 16/3 n^3 flops per matrix x matrices / the label's summed CUDA-event time; "
-                            "'reduction' sums the labels k_hetrd_panel, k_hetrd_her2k and the unblocked tail k_hetrd; "
-                            "traffic = ncu DRAM bytes per matrix (profiles/) x matrices per launch"}
+        if "k_hetrd_panel" in prof:
+            pms, plaunch = prof["k_hetrd_panel"]
+            bpm = _panel_bytes_per_matrix(n)
+            achieved = bpm * solves * args.steps / (pms * 1e-3) / 1e9
+            tr = _traffic_per_matrix("k_hetrd_panel", n)
+            roof = {"bound": "hbm", "kernel": "k_hetrd_panel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                    "frac": achieved / hbm,
+                    "traffic": tr * solves * args.steps / plaunch if tr else None,
+                    "peak_source": hbm_src, "share_of_gpu_time": pms / total_ms, "launches": plaunch,
+                    "note": "algorithmic bytes = the stored triangle of the leading c x c block read once per "
+                            "reduced column c (16 c(c+1)/2 B), summed over the panel columns, x matrices / the "
+                            "label's summed CUDA-event time; traffic = ncu DRAM bytes per matrix (profiles/) x "
+                            "matrices per launch"}
+        # the reduction as a whole against the FP64 peak (algorithmic flops)
+        red = _with_reduction(prof).get("reduction")
+        red_roof = None
+        if red:
+            achieved = _kernel_flops_per_matrix("reduction", n) * solves * args.steps / (red[0] * 1e-3) / 1e12
+            red_roof = {"bound": "fp64", "kernels": "k_hetrd_panel + k_hetrd_her2k + k_hetrd", "achieved": achieved,
+                        "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                        "peak_source": "measured in this run: FP64 FMA throughput probe (MEASURED_PEAKS.json "
+                                       "holds no FP64 figure)",
+                        "share_of_gpu_time": red[0] / total_ms,
+                        "note": "16/3 n^3 flops per matrix (LAPACK zhetrd count)"}
         eig_ms = sum(prof.get(k, (0, 0))[0] for k in EIG_LABELS)
         eig_tf = 13.33 * n ** 3 * solves * args.steps / (eig_ms * 1e-3) / 1e12
         # HBM-bound stages (a) assembly and (c) links / plaquettes: algorithmic bytes per step
@@ -805,6 +825,7 @@ def run_headline(args):
             "mixed": mixed,
             "parity": par,
             "roofline": roof,
+            "reduction_roofline": red_roof,
             "eigensolve_roofline": {"flops_per_solve": "13.33 n^3",
                                     "kernels": "hetrd_panel+hetrd_her2k+hetrd+stebz+stein+larft+ormtr",
                                     "achieved_tflops": eig_tf, "peak_tflops": fp64_peak, "frac": eig_tf / fp64_peak},

@@ -72,17 +72,18 @@ int rlmb_set_refinement_steps(rlmb_context* ctx, int steps);
 /* Eigensolver launch choices (no counterpart in the reference, whose solver is a library
  * call).  With autotuning on, the first eigensolve of each order n in 64..1024 and precision
  * mode on the context times every feasible configuration -- unblocked or blocked reduction,
- * 256- or 512-thread panels, register-resident or GEMM back-transformation, 64- or 128-row
- * tiles of the double-precision X update -- on copies of up to 2 x SMs of the call's own
- * matrices and keeps the fastest for later calls of that order.  rlmb_heev_config reports the
- * configuration used for (n, precision) (the tuned one, or the built-in one) and returns 1 if
- * it was tuned or set, 0 if built-in; rlmb_set_heev_config pins one (-1 / 0 = built-in choice
- * for that item).  panel_threads 0 means the built-in choice. */
+ * 256- or 512-thread panels, register-resident or GEMM back-transformation, 64- or
+ * 128-reflector blocks and 64- or 128-row tiles of the double-precision X update of the
+ * latter -- on copies of up to 2 x SMs of the call's own matrices and keeps the fastest for
+ * later calls of that order.  rlmb_heev_config reports the configuration used for
+ * (n, precision) (the tuned one, or the built-in one) and returns 1 if it was tuned or set,
+ * 0 if built-in; rlmb_set_heev_config pins one (-1 / 0 = built-in choice for that item).
+ * panel_threads, x_tile and bt_block 0 mean the built-in choice. */
 int rlmb_set_autotune(rlmb_context* ctx, int on);
 int rlmb_heev_config(rlmb_context* ctx, int n, int precision, int* blocked, int* gemm_bt, int* panel_threads,
-                     int* x_tile, double* ms_per_matrix);
+                     int* x_tile, int* bt_block, double* ms_per_matrix);
 int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int blocked, int gemm_bt, int panel_threads,
-                         int x_tile);
+                         int x_tile, int bt_block);
 
 /* ------------------------------------------------- (b) Hermitian eigensolver
  * Batched full eigendecomposition, double precision, in place.

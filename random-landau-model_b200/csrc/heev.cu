@@ -1079,12 +1079,17 @@ k_ormtr(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __rest
 
 // ------------------------------------------------ back-transformation for large orders
 // For orders whose 16-reflector blocks do not fit the register/shared-memory scheme of
-// k_ormtr, X = Q Z is applied with blocks of BT_NB = 64 reflectors as two tiled complex
-// GEMMs per block (LAPACK zlarfb restated): W' = T (V^H X), then X -= V W'.  X lives in
-// global memory (column-major, column = eigenvector) and is read twice and written once
-// per block.
+// k_ormtr, X = Q Z is applied with blocks of BT_NB = 64 reflectors (or 128, a tuning choice)
+// as tiled complex GEMMs per block (LAPACK zlarfb restated): W' = T (V^H X), then
+// X -= V W'.  X lives in global memory (column-major, column = eigenvector) and is read twice
+// and written once per block.
 static constexpr int BT_NB = 64;
 static constexpr int BT_GEMM_MIN = 256;   // order from which the GEMM back-transformation runs
+// Blocks of 128 reflectors (T from two 64-reflector halves, k_larft128) halve the passes
+// over X, but at order 3000 they were no faster in double precision and 10 % slower in single
+// precision (the block GEMMs are bound by the tensor pipes, not by X's traffic): they are a
+// tuning choice (HeevTune::bt_nb, rlmb_set_heev_config), not the built-in one.
+static constexpr int BT128_MIN = 1 << 30;
 
 // T factor of block j (reflectors 64j .. 64j+63) of one matrix from its Gram matrix
 // G = V_j^H V_j (column-major 64 x 64, computed by a batched GEMM into the same slot of Tw):
@@ -1122,6 +1127,89 @@ k_larft64(const typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restri
         const int k = idx / BT_NB, c = idx % BT_NB;
         blk[idx] = c <= k ? S[k][c] : cz<C>();
     }
+}
+
+// T factor of a block of 128 reflectors (128j .. 128j+127) from its 128 x 128 Gram matrix
+// G = V^H V (column-major, in the block's slot of Tw), written back row-major:
+//   T = [[T1, 0], [T21, T2]],   T21 = -T2 (G21 T1),   G21 = V2^H V1,
+// where T1 and T2 are the T factors of the two halves (the k_larft64 recurrence, run on both
+// at once by the two halves of the CTA) -- the same matrix the zlarft recurrence gives for
+// all 128 reflectors.  Grid (blocks, matrices), 256 threads; shared memory: S1, S2 (the
+// halves' recurrence tables as in k_larft64) and Y (G21, then G21 T1).
+template <class R>
+__global__ void __launch_bounds__(256)
+k_larft128(const typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ Tw, int n) {
+    typedef typename Cx<R>::T C;
+    constexpr int H = 64, B = 128;
+    typedef C Row[H + 1];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Row* S1 = reinterpret_cast<Row*>(smem_raw);
+    Row* S2 = S1 + H;
+    Row* Y = S2 + H;
+    const int j = blockIdx.x, tid = threadIdx.x;
+    const size_t mat = blockIdx.y;
+    const C* tau = TAU + mat * n;
+    const int nblk = (n - 1 + B - 1) / B;
+    const int i0 = j * B;
+    C* blk = Tw + (mat * nblk + j) * B * B;
+    // S1[l][k] = G(k, l), S2[l][k] = G(64 + k, 64 + l), Y[k][l] = G21(k, l) = G(64 + k, l)
+    for (int idx = tid; idx < H * H; idx += 256) {
+        const int a = idx / H, b = idx % H;
+        S1[a][b] = blk[(size_t)a * B + b];
+        S2[a][b] = blk[(size_t)(H + a) * B + H + b];
+        Y[b][a] = blk[(size_t)a * B + H + b];
+    }
+    __syncthreads();
+    {
+        const int half = tid >> 7, q = (tid & 127) >> 1, h = tid & 1;
+        Row* S = half ? S2 : S1;
+        const int ib = i0 + H * half;
+        for (int k = 0; k < H; ++k) {
+            const int ik = ib + k;
+            const C tk = ik <= n - 2 ? tau[ik] : cz<C>();
+            C sum = cz<C>();
+            if (q < k)
+                for (int l = q + h; l < k; l += 2) cfma(sum, S[l][k], S[l][q]);
+            sum = cadd(sum, shfl_xor(sum, 1));
+            if (h == 0 && q <= k) S[k][q] = q == k ? tk : cscale(cmul(tk, sum), (R)-1);
+            __syncthreads();
+        }
+    }
+    // thread: row k of the 64 x 64 products, columns q = c4 + 4 i
+    const int k = tid >> 2, c4 = tid & 3;
+    C acc[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[i] = cz<C>();
+    // Y <- G21 T1: (G21 T1)[k][q] = sum_{l >= q} G21[k][l] T1[l][q], T1[l][q] = S1[l][q]
+    for (int l = 0; l < H; ++l) {
+        const C g = Y[k][l];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int q = c4 + 4 * i;
+            if (l >= q) cfma(acc[i], g, S1[l][q]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) Y[k][c4 + 4 * i] = acc[i];
+    __syncthreads();
+    // T21 = -T2 Y: T21[k][q] = -sum_{l <= k} T2[k][l] Y[l][q], T2[k][l] = S2[k][l]
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[i] = cz<C>();
+    for (int l = 0; l <= k; ++l) {
+        const C t2 = S2[k][l];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) cfma(acc[i], t2, Y[l][c4 + 4 * i]);
+    }
+    // row-major T: rows 0..63 [T1 0], rows 64..127 [T21 T2]
+    for (int idx = tid; idx < H * H; idx += 256) {
+        const int a = idx / H, b = idx % H;
+        blk[(size_t)a * B + b] = b <= a ? S1[a][b] : cz<C>();
+        blk[(size_t)a * B + H + b] = cz<C>();
+        blk[(size_t)(H + a) * B + H + b] = b <= a ? S2[a][b] : cz<C>();
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) blk[(size_t)(H + k) * B + c4 + 4 * i] = cscale(acc[i], (R)-1);
 }
 
 // Z (row-major real) -> X (column-major complex), grid-stride over all batch entries.
@@ -1201,15 +1289,15 @@ struct OpReflH {
     }
 };
 
-// Gram matrices of all 64-reflector blocks in one batched GEMM: batch index z = mat * nblk
-// + j; A(q, r) = conj(v_{64j+q}[r]), B(r, l) = v_{64j+l}[r].
+// Gram matrices of all blocks of bs reflectors in one batched GEMM: batch index z = mat * nblk
+// + j; A(q, r) = conj(v_{bs j+q}[r]), B(r, l) = v_{bs j+l}[r].
 template <class C>
 struct OpBlkReflH {
     static constexpr bool RFAST = false;
     const C* a;
-    int n, nblk;
+    int n, nblk, bs;
     __device__ __forceinline__ C elem(size_t z, int q, int r) const {
-        C v = refl_entry(a + (z / nblk) * (size_t)n * n, n, (int)(z % nblk) * BT_NB + q, r);
+        C v = refl_entry(a + (z / nblk) * (size_t)n * n, n, (int)(z % nblk) * bs + q, r);
         v.y = -v.y;
         return v;
     }
@@ -1218,9 +1306,9 @@ template <class C>
 struct OpBlkRefl {
     static constexpr bool KFAST = true;
     const C* a;
-    int n, nblk;
+    int n, nblk, bs;
     __device__ __forceinline__ C elem(size_t z, int r, int l) const {
-        return refl_entry(a + (z / nblk) * (size_t)n * n, n, (int)(z % nblk) * BT_NB + l, r);
+        return refl_entry(a + (z / nblk) * (size_t)n * n, n, (int)(z % nblk) * bs + l, r);
     }
 };
 
@@ -1999,6 +2087,7 @@ struct HeevTune {
     int gemm_bt = -1;    // 1: GEMM back-transformation, 0: register-resident k_ormtr (where it fits)
     int panel_nt = 0;    // threads per panel CTA, 256 or 512
     int xtile = 0;       // row tile of the double-precision X -= V W' update, 64 or 128
+    int bt_nb = 0;       // reflectors per block of the GEMM back-transformation, 64 or 128
 };
 
 // Shape of one eigensolve chunk: kernel configurations and the scratch layout per matrix
@@ -2014,7 +2103,7 @@ struct HeevPlan {
     bool small_bt;       // k_ormtr (register-resident Z chunk) or the blocked GEMM path
     int ch, dbuf;
     size_t smem_orm;
-    int nblk16, nblk64;
+    int nblk16, bt_nb, nblkbt;   // k_ormtr blocks; GEMM back-transformation block size and count
     int npanels, m_tail;  // blocked reduction: panels of HP_W columns, then k_hetrd on m_tail
     int panel_nt, xtile;  // tuned launch choices (0: built-in)
     // per: bytes per matrix of the chunk's regions (offsets off_*, times the chunk size);
@@ -2040,7 +2129,8 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.hc = mixed ? hetrd_config<float>(p.m_tail) : hetrd_config<double>(p.m_tail);
     p.smem_tri = 4 * (size_t)n * sizeof(double) + n * sizeof(int);
     p.nblk16 = (n - 1 + ORM_NB - 1) / ORM_NB;
-    p.nblk64 = (n - 1 + BT_NB - 1) / BT_NB;
+    p.bt_nb = tune.bt_nb ? tune.bt_nb : n >= BT128_MIN ? 2 * BT_NB : BT_NB;
+    p.nblkbt = (n - 1 + p.bt_nb - 1) / p.bt_nb;
     int ch = 16;
     while (ch > 1 && (n + 256 / ch - 1) / (256 / ch) > ORM_RPT) ch >>= 1;
     p.ch = ch;
@@ -2065,8 +2155,8 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.off_z = off; off += r256(nn * sizeof(double));
     p.off_lu = off; off += r256(5 * (size_t)n * TRI_THREADS * sizeof(double));
     p.off_x = off; off += r256(nn * ce);
-    p.off_t = off; off += r256((p.small_bt ? (size_t)p.nblk16 * ORM_NB * ORM_NB : (size_t)p.nblk64 * BT_NB * BT_NB) * ce);
-    p.off_w = off; off += p.small_bt ? 0 : r256(2 * (size_t)BT_NB * n * ce);   // G and W' of a block
+    p.off_t = off; off += r256((p.small_bt ? (size_t)p.nblk16 * ORM_NB * ORM_NB : (size_t)p.nblkbt * p.bt_nb * p.bt_nb) * ce);
+    p.off_w = off; off += p.small_bt ? 0 : r256(2 * (size_t)p.bt_nb * n * ce);   // G and W' of a block
     p.off_res = 0;   // (the refinement regions: per2 below)
     p.off_x1 = 0;
     p.off_cl = off; off += mixed ? r256(n * sizeof(int2)) : 0;
@@ -2089,7 +2179,7 @@ size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n, false).per; }
 size_t heev_max_chunk(int n) {
     const HeevPlan p = heev_plan(n, false);
     size_t c = 65535;
-    if (!p.small_bt) c = std::min<size_t>(c, 65535 / std::max(p.nblk64, 1));
+    if (!p.small_bt) c = std::min<size_t>(c, 65535 / std::max(p.nblkbt, 1));
     return c;
 }
 
@@ -2183,47 +2273,54 @@ static int back_transform(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         RLMB_CHUNK_LAUNCHED();
         return RLMB_OK;
     }
+    const int bs = p.bt_nb, nblk = p.nblkbt;
     RLMB_CHUNK_PROF("k_larft");
-    if (launch_work_gemm<C, 64>(st, OpBlkReflH<C>{Aw, n, p.nblk64}, OpBlkRefl<C>{Aw, n, p.nblk64},
-                            EpStore<C>{Tw, BT_NB, (size_t)BT_NB * BT_NB}, BT_NB, BT_NB, n, nb * p.nblk64) != cudaSuccess)
+    if (launch_work_gemm<C, 64>(st, OpBlkReflH<C>{Aw, n, nblk, bs}, OpBlkRefl<C>{Aw, n, nblk, bs},
+                            EpStore<C>{Tw, bs, (size_t)bs * bs}, bs, bs, n, nb * nblk) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
-    const size_t smem_t = BT_NB * (BT_NB + 1) * sizeof(C);
-    if (cudaFuncSetAttribute(k_larft64<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess)
-        return RLMB_ERR_CUDA;
     RLMB_CHUNK_PROF("k_larft");
-    k_larft64<R><<<dim3(p.nblk64, nb), 2 * BT_NB, smem_t, st>>>(TAUw, Tw, n);
+    if (bs == BT_NB) {
+        const size_t smem_t = BT_NB * (BT_NB + 1) * sizeof(C);
+        if (cudaFuncSetAttribute(k_larft64<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        k_larft64<R><<<dim3(nblk, nb), 2 * BT_NB, smem_t, st>>>(TAUw, Tw, n);
+    } else {
+        const size_t smem_t = 3 * BT_NB * (BT_NB + 1) * sizeof(C);
+        if (cudaFuncSetAttribute(k_larft128<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        k_larft128<R><<<dim3(nblk, nb), 256, smem_t, st>>>(TAUw, Tw, n);
+    }
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ormtr");
     k_z_to_x<C><<<2048, 256, 0, st>>>(Zw, Xw, n, (size_t)nb * nn);
     RLMB_CHUNK_LAUNCHED();
-    // per block j of 64 reflectors (zlarfb): G = V^H X, W' = T G, X -= V W'; G and W' are
-    // [n][64] per matrix (column c of G at c*64)
+    // per block j of bs reflectors (zlarfb): G = V^H X, W' = T G, X -= V W'; G and W' are
+    // [n][bs] per matrix (column c of G at c*bs)
     C* G = Wp;
-    C* W2 = Wp + (size_t)nb * BT_NB * n;
-    const size_t gs = (size_t)BT_NB * n;
-    for (int j = 0; j < p.nblk64; ++j) {
-        const int i0 = j * BT_NB;
-        const int rows = std::min(i0 + BT_NB - 1, n - 2) + 1;   // rows 0..i1 carry the block
+    C* W2 = Wp + (size_t)nb * bs * n;
+    const size_t gs = (size_t)bs * n;
+    for (int j = 0; j < nblk; ++j) {
+        const int i0 = j * bs;
+        const int rows = std::min(i0 + bs - 1, n - 2) + 1;   // rows 0..i1 carry the block
         RLMB_CHUNK_PROF("k_ormtr");
-        if (launch_work_gemm<C, 64>(st, OpReflH<C>{Aw, n, i0}, OpColB<C, C>{Xw, n, nn}, EpStore<C>{G, BT_NB, gs},
-                                BT_NB, n, rows, nb) != cudaSuccess)
+        if (launch_work_gemm<C, 64>(st, OpReflH<C>{Aw, n, i0}, OpColB<C, C>{Xw, n, nn}, EpStore<C>{G, bs, gs},
+                                bs, n, rows, nb) != cudaSuccess)
             return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
         RLMB_CHUNK_PROF("k_ormtr");
-        if (launch_work_gemm<C, 64>(st, OpRowA<C, C, false>{Tw + (size_t)j * BT_NB * BT_NB, BT_NB,
-                                                        (size_t)p.nblk64 * BT_NB * BT_NB},
-                                OpColB<C, C>{G, BT_NB, gs}, EpStore<C>{W2, BT_NB, gs}, BT_NB, n, BT_NB, nb) != cudaSuccess)
+        if (launch_work_gemm<C, 64>(st, OpRowA<C, C, false>{Tw + (size_t)j * bs * bs, bs, (size_t)nblk * bs * bs},
+                                OpColB<C, C>{G, bs, gs}, EpStore<C>{W2, bs, gs}, bs, n, bs, nb) != cudaSuccess)
             return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
         RLMB_CHUNK_PROF("k_ormtr");
         // X -= V W': 64-row tiles (two CTAs per SM) on the DMMA engine unless tuned to 128
         // (the tcgen05 engine of the single-precision mode has its own tile)
         const cudaError_t ex =
-            p.xtile == 128 ? launch_work_gemm<C, 128>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs},
-                                                      EpSub<C>{Xw, n}, rows, n, BT_NB, nb)
-                           : launch_work_gemm<C, 64>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, BT_NB, gs},
-                                                     EpSub<C>{Xw, n}, rows, n, BT_NB, nb);
+            p.xtile == 128 ? launch_work_gemm<C, 128>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, bs, gs},
+                                                      EpSub<C>{Xw, n}, rows, n, bs, nb)
+                           : launch_work_gemm<C, 64>(st, OpRefl<C>{Aw, n, i0}, OpColB<C, C>{W2, bs, gs},
+                                                     EpSub<C>{Xw, n}, rows, n, bs, nb);
         if (ex != cudaSuccess) return RLMB_ERR_CUDA;
         RLMB_CHUNK_LAUNCHED();
     }
@@ -2416,8 +2513,8 @@ using namespace rlmb;
 // ----------------------------------------------------------------------- autotuner
 // Per context, per (order, precision): the launch choices of HeevTune picked by timing every
 // feasible candidate -- unblocked or blocked reduction (from order 128), 256- or 512-thread
-// panels, register-resident or GEMM back-transformation, 64- or 128-row X-update tiles (double
-// precision) -- on copies of up to 2 x SMs of the call's own matrices (at most 2 GB of them),
+// panels, register-resident or GEMM back-transformation, 64- or 128-reflector blocks and 64- or
+// 128-row X-update tiles (double precision) of the latter -- on copies of up to 2 x SMs of the call's own matrices (at most 2 GB of them),
 // each candidate run twice and timed the second time with CUDA events.  Orders 64 .. 1024
 // are tuned; others keep the built-in choices.
 struct TuneEntry {
@@ -2441,17 +2538,20 @@ static std::vector<HeevTune> tune_candidates(int n, bool mixed) {
         for (int gemm = 0; gemm <= 1; ++gemm)
             for (int nt : {256, 512}) {
                 if (!blocked && nt == 256) continue;   // no panels: one entry
-                for (int xt : {64, 128}) {
-                    if ((!gemm || mixed) && xt == 128) continue;
-                    HeevTune t;
-                    t.blocked = blocked;
-                    t.gemm_bt = gemm;
-                    t.panel_nt = blocked ? nt : 0;
-                    t.xtile = gemm && !mixed ? xt : 0;
-                    const HeevPlan p = heev_plan(n, mixed, 2, -1, t);
-                    if (!gemm && !p.small_bt) continue;   // register back-transformation does not fit
-                    out.push_back(t);
-                }
+                for (int xt : {64, 128})
+                    for (int bs : {64, 128}) {
+                        if ((!gemm || mixed) && xt == 128) continue;
+                        if (!gemm && bs == 128) continue;
+                        HeevTune t;
+                        t.blocked = blocked;
+                        t.gemm_bt = gemm;
+                        t.panel_nt = blocked ? nt : 0;
+                        t.xtile = gemm && !mixed ? xt : 0;
+                        t.bt_nb = gemm ? bs : 0;
+                        const HeevPlan p = heev_plan(n, mixed, 2, -1, t);
+                        if (!gemm && !p.small_bt) continue;   // register back-transformation does not fit
+                        out.push_back(t);
+                    }
             }
     }
     return out;
@@ -2562,7 +2662,7 @@ int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n,
     size_t nb2 = per2 ? std::max<size_t>(1, std::min<size_t>((size_t)batch, budget / 8 / per2)) : 0;
     size_t chunk = std::max<size_t>(1, std::min<size_t>((budget - nb2 * per2) / per, (size_t)batch));
     chunk = std::min<size_t>(chunk, 65535);   // grid y / z extent of the per-matrix launches
-    if (!plan.small_bt) chunk = std::min<size_t>(chunk, 65535 / std::max(plan.nblk64, 1));   // (matrix, block) batches
+    if (!plan.small_bt) chunk = std::min<size_t>(chunk, 65535 / std::max(plan.nblkbt, 1));   // (matrix, block) batches
     // equal chunks: a short last chunk would leave most SMs idle in the one-CTA-per-matrix kernels
     const size_t nchunks = (batch + chunk - 1) / chunk;
     chunk = (batch + nchunks - 1) / nchunks;
@@ -2594,7 +2694,7 @@ extern "C" int rlmb_set_autotune(rlmb_context* ctx, int on) {
 }
 
 extern "C" int rlmb_heev_config(rlmb_context* ctx, int n, int precision, int* blocked, int* gemm_bt,
-                                int* panel_threads, int* x_tile, double* ms_per_matrix) {
+                                int* panel_threads, int* x_tile, int* bt_block, double* ms_per_matrix) {
     if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED)) return RLMB_ERR_ARG;
     auto& tc = tune_cache(ctx);
     auto it = tc.find({n, precision});
@@ -2609,21 +2709,23 @@ extern "C" int rlmb_heev_config(rlmb_context* ctx, int n, int precision, int* bl
     if (gemm_bt) *gemm_bt = !p.small_bt;
     if (panel_threads) *panel_threads = p.panel_nt;
     if (x_tile) *x_tile = p.xtile == 128 ? 128 : 64;
+    if (bt_block) *bt_block = p.bt_nb;
     if (ms_per_matrix) *ms_per_matrix = ms;
     return it != tc.end() ? 1 : 0;
 }
 
 extern "C" int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int blocked, int gemm_bt,
-                                    int panel_threads, int x_tile) {
+                                    int panel_threads, int x_tile, int bt_block) {
     if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED) || blocked < -1 ||
         blocked > 1 || gemm_bt < -1 || gemm_bt > 1 || (panel_threads != 0 && panel_threads != 256 && panel_threads != 512) ||
-        (x_tile != 0 && x_tile != 64 && x_tile != 128))
+        (x_tile != 0 && x_tile != 64 && x_tile != 128) || (bt_block != 0 && bt_block != 64 && bt_block != 128))
         return RLMB_ERR_ARG;
     HeevTune t;
     t.blocked = blocked;
     t.gemm_bt = gemm_bt;
     t.panel_nt = panel_threads;
     t.xtile = x_tile;
+    t.bt_nb = bt_block;
     tune_cache(ctx)[{n, precision}] = TuneEntry{t, 0.0};
     return RLMB_OK;
 }

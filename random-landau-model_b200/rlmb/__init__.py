@@ -38,9 +38,9 @@ _SIGNATURES = {
     "rlmb_heevd_host": (ctypes.c_int, [_vp, _c_dp, _c_dp, ctypes.c_int, ctypes.c_int]),
     "rlmb_heevd_batched_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "rlmb_set_autotune": (ctypes.c_int, [_vp, ctypes.c_int]),
-    "rlmb_heev_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip, _c_ip, _c_ip, _c_ip, _c_dp]),
+    "rlmb_heev_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip, _c_ip, _c_ip, _c_ip, _c_ip, _c_dp]),
     "rlmb_set_heev_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                            ctypes.c_int, ctypes.c_int]),
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "rlmb_zgemm_batched": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int]),
     "rlmb_tc_fault_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
@@ -255,19 +255,19 @@ class Context:
         _check(lib().rlmb_set_autotune(self.h, 1 if on else 0), "rlmb_set_autotune")
 
     def heev_config(self, n, precision=None):
-        """(tuned, {blocked, gemm_bt, panel_threads, x_tile, ms_per_matrix}) used for order n."""
+        """(tuned, {blocked, gemm_bt, panel_threads, x_tile, bt_block, ms_per_matrix}) used for order n."""
         prec = self.precision if precision is None else precision
-        vals = [ctypes.c_int() for _ in range(4)]
+        vals = [ctypes.c_int() for _ in range(5)]
         ms = ctypes.c_double()
         rc = lib().rlmb_heev_config(self.h, n, prec, *[ctypes.byref(v) for v in vals], ctypes.byref(ms))
         if rc < 0:
             _check(rc, "rlmb_heev_config")
-        keys = ("blocked", "gemm_bt", "panel_threads", "x_tile")
+        keys = ("blocked", "gemm_bt", "panel_threads", "x_tile", "bt_block")
         return rc == 1, dict(zip(keys, [v.value for v in vals]), ms_per_matrix=ms.value)
 
-    def set_heev_config(self, n, blocked=-1, gemm_bt=-1, panel_threads=0, x_tile=0, precision=None):
+    def set_heev_config(self, n, blocked=-1, gemm_bt=-1, panel_threads=0, x_tile=0, bt_block=0, precision=None):
         prec = self.precision if precision is None else precision
-        _check(lib().rlmb_set_heev_config(self.h, n, prec, blocked, gemm_bt, panel_threads, x_tile),
+        _check(lib().rlmb_set_heev_config(self.h, n, prec, blocked, gemm_bt, panel_threads, x_tile, bt_block),
                "rlmb_set_heev_config")
 
     GEMM_FP64, GEMM_TF32X3, GEMM_TF32X3_F64ACC = 0, 1, 2

@@ -444,10 +444,37 @@ def test_heevd_every_launch_configuration(n):
             for gemm in (0, 1):
                 for nt in (256, 512):
                     for xt in (64, 128):
-                        c.set_heev_config(n, blocked, gemm, nt, xt)
-                        w, X = _run_heevd(c, mats)
-                        for b, M in enumerate(mats):
-                            _check_eig(M, w[b], X[b], np.linalg.eigvalsh(M))
+                        for bs in ((64, 128) if gemm else (0,)):
+                            c.set_heev_config(n, blocked, gemm, nt, xt, bs)
+                            w, X = _run_heevd(c, mats)
+                            for b, M in enumerate(mats):
+                                _check_eig(M, w[b], X[b], np.linalg.eigvalsh(M))
+    finally:
+        c.close()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+@pytest.mark.parametrize("n,bs", [(1000, 128), (1000, 64), (1600, 0), (300, 128), (385, 128)])
+def test_heevd_back_transformation_blocks(n, bs, mixed):
+    """The GEMM back-transformation in blocks of 128 reflectors (T from two 64-reflector halves)
+    against 64, at orders whose last block is partial in either half; 0 = the built-in choice
+    (64)."""
+    import rlmb
+    c = rlmb.Context(0)
+    try:
+        if mixed:
+            c.precision = c.MIXED
+        c.set_heev_config(n, 1, 1, 0, 0, bs)
+        assert c.heev_config(n)[1]["bt_block"] == (bs or 64)
+        rng = np.random.default_rng(n + bs)
+        mats = [_hermitian(rng, n) for _ in range(2)]
+        w, X = _run_heevd(c, mats)
+        tol = 1e-10 if mixed else 1e-12   # the mixed mode's bound (test_gpu_mixed) or FP64's
+        for b, M in enumerate(mats):
+            wref = np.linalg.eigvalsh(M)
+            assert np.abs(w[b] - wref).max() <= tol * np.abs(wref).max()
+            assert np.linalg.norm(M @ X[b] - X[b] * w[b][None, :]) <= tol * np.linalg.norm(M)
+            assert np.linalg.norm(X[b].conj().T @ X[b] - np.eye(n)) <= (1e-10 if mixed else 1e-11)
     finally:
         c.close()
 
