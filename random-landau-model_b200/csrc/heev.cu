@@ -1464,6 +1464,116 @@ __device__ __forceinline__ void hemv_upper(const C* __restrict__ a, int ld, int 
     }
 }
 
+// Loads of the panel pairs V, W: through L1 (ld) when one CTA owns the matrix for the whole
+// panel, around it (ld.global.cg) when other CTAs wrote them during the same launch.
+template <bool CG, class C>
+__device__ __forceinline__ C pv_ld(const C* p) {
+    if constexpr (CG) return __ldcg(p);
+    else return *p;
+}
+
+// Column j of the panel (column c = m - 1 - j of the leading m x m block) of matrix mat, by
+// the NT threads of one CTA; vn, pn, coef, red: the CTA's shared work arrays.
+template <int NT, class R, bool CG>
+__device__ __forceinline__ void panel_column(typename Cx<R>::T* __restrict__ A, double* __restrict__ D,
+                                             double* __restrict__ E, typename Cx<R>::T* __restrict__ TAU,
+                                             typename Cx<R>::T* __restrict__ PV, typename Cx<R>::T* __restrict__ PW,
+                                             int n, int m, size_t mat, int j, typename Cx<R>::T* vn,
+                                             typename Cx<R>::T* pn, typename Cx<R>::T* coef, R* red) {
+    typedef typename Cx<R>::T C;
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    GlobalStore<C> gs{A + mat * (size_t)n * n, n};
+    double* dd = D + mat * n;
+    double* ee = E + mat * n;
+    C* tt = TAU + mat * n;
+    C* V = PV + mat * (size_t)HP_W * n;   // pair q at V + q*n, W + q*n
+    C* W = PW + mat * (size_t)HP_W * n;
+    if (m == n && j == 0 && tid == 0) {
+        ee[n - 1] = 0.0;
+        tt[n - 1] = cz<C>();
+    }
+    const int c = m - 1 - j;
+    // (1) column c brought up to date with the panel's pairs q < j
+    R part = 0;
+    for (int r = tid; r <= c; r += NT) {
+        C x = *gs.at(r, c);
+        for (int q = 0; q < j; ++q) {
+            const C* vq = V + (size_t)q * n;
+            const C* wq = W + (size_t)q * n;
+            C u = cmul(pv_ld<CG>(vq + r), cconj(pv_ld<CG>(wq + c)));
+            cfma(u, pv_ld<CG>(wq + r), cconj(pv_ld<CG>(vq + c)));
+            x = csub(x, u);
+        }
+        if (r == c) x.y = 0;
+        vn[r] = x;
+        if (r < c - 1) part += cabs2(x);
+        if (r < c) pn[r] = cz<C>();
+    }
+    const R xn2 = block_sum<NT>(part, red);
+    // (2) reflector of step c-1: alpha = A'[c-1][c], x = A'[0..c-2][c]
+    R beta;
+    C tau, scal;
+    reflector(vn[c - 1], xn2, beta, tau, scal);
+    const bool act = !(tau.x == 0 && tau.y == 0);
+    __syncthreads();
+    if (tid == 0) dd[c] = vn[c].x;
+    for (int r = tid; r < c - 1; r += NT) {
+        const C x = act ? cmul(scal, vn[r]) : vn[r];
+        vn[r] = x;
+        *gs.at(r, c) = x;
+    }
+    if (tid == 0) {
+        vn[c - 1] = cm<C>(1, 0);
+        *gs.at(c - 1, c) = cm<C>(beta, 0);
+        ee[c - 1] = beta;
+        tt[c - 1] = tau;
+    }
+    __syncthreads();
+    // (3) pn = A v over the stored leading c x c block (read only)
+    if (act) hemv_upper<NT>(gs.a, n, c, vn, pn);
+    // (4) w_q^H v (even slots) and v_q^H v (odd slots) for q < j
+    for (int t2 = warp; t2 < 2 * j; t2 += NW) {
+        const int q = t2 >> 1;
+        const C* y = (t2 & 1) ? V + (size_t)q * n : W + (size_t)q * n;
+        C sd = cz<C>();
+        for (int r = lane; r < c; r += 32) cfmac(sd, pv_ld<CG>(y + r), vn[r]);
+        sd = warp_sum(sd);
+        if (lane == 0) coef[t2] = sd;
+    }
+    __syncthreads();
+    // (5) x = tau (pn - sum_q V_q (w_q^H v) + W_q (v_q^H v)); w = x - tau/2 (x^H v) v
+    C dpart = cz<C>();
+    for (int r = tid; r < c; r += NT) {
+        C x = pn[r];
+        for (int q = 0; q < j; ++q) {
+            C u = cmul(pv_ld<CG>(V + (size_t)q * n + r), coef[2 * q]);
+            cfma(u, pv_ld<CG>(W + (size_t)q * n + r), coef[2 * q + 1]);
+            x = csub(x, u);
+        }
+        x = cmul(tau, x);
+        pn[r] = x;
+        cfmac(dpart, x, vn[r]);
+    }
+    const C xv = block_sum_c<NT>(dpart, red);
+    const C al = cscale(cmul(tau, xv), (R)-0.5);
+    C* vj = V + (size_t)j * n;
+    C* wj = W + (size_t)j * n;
+    for (int r = tid; r < c; r += NT) {
+        vj[r] = vn[r];
+        wj[r] = act ? cadd(pn[r], cmul(al, vn[r])) : cz<C>();
+    }
+    __syncthreads();
+}
+
+// Shared work arrays of the panel kernels: vn [m] (column / reflector), pn [m] (A' v
+// accumulator), coef [2*HP_W] (w_q^H v, v_q^H v), red [2*warps].
+template <int NT, class R>
+__host__ __device__ constexpr size_t panel_smem(int m) {
+    return (2 * (size_t)m + 2 * HP_W) * sizeof(typename Cx<R>::T) + 2 * (NT / 32) * sizeof(R);
+}
+
+// One CTA per matrix: the panel's HP_W columns in order.
 template <int NT, class R>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
 k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
@@ -1471,95 +1581,84 @@ k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double*
               typename Cx<R>::T* __restrict__ PW, int n, int m) {
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* vn = reinterpret_cast<C*>(smem_raw);   // [m] column / reflector
-    C* pn = vn + m;                            // [m] A' v accumulator
-    C* coef = pn + m;                          // [2*HP_W] w_q^H v, v_q^H v
-    R* red = reinterpret_cast<R*>(coef + 2 * HP_W);   // [2*warps]
-    constexpr int NW = NT / 32;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const size_t mat = blockIdx.x;
-    GlobalStore<C> gs{A + mat * (size_t)n * n, n};
-    double* dd = D + mat * n;
-    double* ee = E + mat * n;
-    C* tt = TAU + mat * n;
-    C* V = PV + mat * (size_t)HP_W * n;   // pair q at V + q*n, W + q*n
-    C* W = PW + mat * (size_t)HP_W * n;
-    if (m == n && tid == 0) {
-        ee[n - 1] = 0.0;
-        tt[n - 1] = cz<C>();
-    }
-    for (int j = 0; j < HP_W; ++j) {
-        const int c = m - 1 - j;
-        // (1) column c brought up to date with the panel's pairs q < j
-        R part = 0;
-        for (int r = tid; r <= c; r += NT) {
-            C x = *gs.at(r, c);
-            for (int q = 0; q < j; ++q) {
-                const C* vq = V + (size_t)q * n;
-                const C* wq = W + (size_t)q * n;
-                C u = cmul(vq[r], cconj(wq[c]));
-                cfma(u, wq[r], cconj(vq[c]));
-                x = csub(x, u);
-            }
-            if (r == c) x.y = 0;
-            vn[r] = x;
-            if (r < c - 1) part += cabs2(x);
-            if (r < c) pn[r] = cz<C>();
-        }
-        const R xn2 = block_sum<NT>(part, red);
-        // (2) reflector of step c-1: alpha = A'[c-1][c], x = A'[0..c-2][c]
-        R beta;
-        C tau, scal;
-        reflector(vn[c - 1], xn2, beta, tau, scal);
-        const bool act = !(tau.x == 0 && tau.y == 0);
-        __syncthreads();
-        if (tid == 0) dd[c] = vn[c].x;
-        for (int r = tid; r < c - 1; r += NT) {
-            const C x = act ? cmul(scal, vn[r]) : vn[r];
-            vn[r] = x;
-            *gs.at(r, c) = x;
-        }
+    C* vn = reinterpret_cast<C*>(smem_raw);
+    C* pn = vn + m;
+    C* coef = pn + m;
+    R* red = reinterpret_cast<R*>(coef + 2 * HP_W);
+    for (int j = 0; j < HP_W; ++j)
+        panel_column<NT, R, false>(A, D, E, TAU, PV, PW, n, m, blockIdx.x, j, vn, pn, coef, red);
+}
+
+// The same panel for chunks of more matrices than SMs: one resident CTA of NT threads per SM
+// (grid <= SMs) takes units (matrix, column) from a queue, unit u = claim - base = matrix
+// u % nb, column u / nb, so that every SM keeps NT threads of loads in flight whatever the
+// number of matrices (one CTA per matrix would leave SMs with a single CTA when the chunk has
+// between one and two matrices per SM).  Column j of a matrix needs column j - 1 (its panel
+// pair): q[2 + mat] counts the columns of each matrix completed in the chunk; a unit waits
+// for done = col0 + j, a wait bounded by TC_WAIT_NS that sets the abort flag q[1] (and counts
+// in g_tc_fault) when it runs out.  The claims of a launch end with one failed claim per CTA,
+// so launch k's units start at base = k * (nb * HP_W + grid).  Units are claimed in order and
+// wait only on earlier claims, which CTAs already running hold: no wait depends on a CTA
+// that has not started.
+template <int NT, class R>
+__global__ void __launch_bounds__(NT, 1)
+k_hetrd_panel_q(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
+                typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ PV,
+                typename Cx<R>::T* __restrict__ PW, int n, int m, int nb, int* q, long long base, int col0,
+                int* __restrict__ info) {
+    typedef typename Cx<R>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* vn = reinterpret_cast<C*>(smem_raw);
+    C* pn = vn + m;
+    C* coef = pn + m;
+    R* red = reinterpret_cast<R*>(coef + 2 * HP_W);
+    __shared__ long long s_unit;
+    __shared__ int s_go;
+    const int tid = threadIdx.x;
+    const long long units = (long long)nb * HP_W;
+    for (;;) {
         if (tid == 0) {
-            vn[c - 1] = cm<C>(1, 0);
-            *gs.at(c - 1, c) = cm<C>(beta, 0);
-            ee[c - 1] = beta;
-            tt[c - 1] = tau;
-        }
-        __syncthreads();
-        // (3) pn = A v over the stored leading c x c block (read only)
-        if (act) hemv_upper<NT>(gs.a, n, c, vn, pn);
-        // (4) w_q^H v (even slots) and v_q^H v (odd slots) for q < j
-        for (int t2 = warp; t2 < 2 * j; t2 += NW) {
-            const int q = t2 >> 1;
-            const C* y = (t2 & 1) ? V + (size_t)q * n : W + (size_t)q * n;
-            C sd = cz<C>();
-            for (int r = lane; r < c; r += 32) cfmac(sd, y[r], vn[r]);
-            sd = warp_sum(sd);
-            if (lane == 0) coef[t2] = sd;
-        }
-        __syncthreads();
-        // (5) x = tau (pn - sum_q V_q (w_q^H v) + W_q (v_q^H v)); w = x - tau/2 (x^H v) v
-        C dpart = cz<C>();
-        for (int r = tid; r < c; r += NT) {
-            C x = pn[r];
-            for (int q = 0; q < j; ++q) {
-                C u = cmul(V[(size_t)q * n + r], coef[2 * q]);
-                cfma(u, W[(size_t)q * n + r], coef[2 * q + 1]);
-                x = csub(x, u);
+            long long u = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(q + 4), 1ull) - base;
+            if (*(volatile int*)(q + 1)) u = units;   // aborted: stop claiming work
+            s_unit = u;
+            s_go = 1;
+            if (u < units && u >= nb) {   // column j > 0: wait for column j - 1 of the matrix
+                const int mat = (int)(u % nb), j = (int)(u / nb);
+                const int* dp = q + 8 + mat;
+                int v;
+                asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(dp) : "memory");
+                if (v < col0 + j) {
+                    const unsigned long long t0 = tc_ns();
+                    for (;;) {
+                        __nanosleep(64);
+                        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(dp) : "memory");
+                        if (v >= col0 + j) break;
+                        if (*(volatile int*)(q + 1) || tc_ns() - t0 > TC_WAIT_NS) {
+                            if (atomicExch(q + 1, 1) == 0) atomicAdd(&g_tc_fault, 1);
+                            if (info) info[mat] = -1;
+                            s_go = 0;
+                            break;
+                        }
+                    }
+                }
             }
-            x = cmul(tau, x);
-            pn[r] = x;
-            cfmac(dpart, x, vn[r]);
-        }
-        const C xv = block_sum_c<NT>(dpart, red);
-        const C al = cscale(cmul(tau, xv), (R)-0.5);
-        C* vj = V + (size_t)j * n;
-        C* wj = W + (size_t)j * n;
-        for (int r = tid; r < c; r += NT) {
-            vj[r] = vn[r];
-            wj[r] = act ? cadd(pn[r], cmul(al, vn[r])) : cz<C>();
         }
         __syncthreads();
+        const long long u = s_unit;
+        const int go = s_go;
+        __syncthreads();
+        if (u >= units || !go) break;
+        __threadfence();
+        const int mat = (int)(u % nb), j = (int)(u / nb);
+        panel_column<NT, R, true>(A, D, E, TAU, PV, PW, n, m, mat, j, vn, pn, coef, red);
+        // every thread's writes of the column, then the release of the column count
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) {
+            const int v = col0 + j + 1;
+            int* dp = q + 8 + mat;
+            asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(dp), "r"(v) : "memory");
+        }
     }
 }
 
@@ -2111,7 +2210,7 @@ struct HeevPlan {
     // refinement uses for one sub-chunk of matrices at a time
     size_t per2, off2_x1;
     size_t off_d, off_e, off_tau, off_a, off_z, off_lu, off_x, off_t, off_w, off_res, off_x1, off_cl,
-        off_y, off_mu, off_st, off_pv, per;
+        off_y, off_mu, off_st, off_pv, off_q, per;
 };
 
 static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1, HeevTune tune = HeevTune{}) {
@@ -2164,6 +2263,7 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.off_mu = off; off += mixed ? r256(n * sizeof(double)) : 0;
     p.off_st = off; off += mixed ? r256(3 * (size_t)n * sizeof(double)) : 0;
     p.off_pv = off; off += p.npanels > 0 ? r256(2 * (size_t)HP_W * n * ce) : 0;   // panel V, W
+    p.off_q = off; off += p.npanels > 0 ? r256(16) : 0;   // panel queue: claims, abort flag, column counts
     p.per = off;
     p.per2 = mixed ? r256(nn * sizeof(cplx)) : 0;                              // residual R
     p.off2_x1 = p.per2;
@@ -2203,34 +2303,41 @@ size_t heev_max_chunk(int n) {
 // the panel pairs of the chunk (V of every matrix, then W of every matrix).
 template <class R>
 static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, int nb, typename Cx<R>::T* A,
-                          double* D, double* E, typename Cx<R>::T* TAU, typename Cx<R>::T* PV,
+                          double* D, double* E, typename Cx<R>::T* TAU, typename Cx<R>::T* PV, int* Q, int* info,
                           long long* launches) {
     typedef typename Cx<R>::T C;
     const int n = p.n;
     int m = n;
     if (p.npanels > 0) {
         C* PWb = PV + (size_t)nb * HP_W * n;
-        // 256 threads (two CTAs per SM) for orders 385..512, 512 threads otherwise (measured);
-        // above order 512 also 256 threads when the chunk has more matrices than SMs but
-        // fits two per SM: all of it is then resident at once instead of in two waves
-        auto smem_of = [&](int nt) { return (2 * (size_t)n + 2 * HP_W) * sizeof(C) + 2 * (nt / 32) * sizeof(R); };
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        // built-in choice above order 512 for chunks of more matrices than SMs: one 512-thread
+        // CTA per SM taking (matrix, column) units from a queue (k_hetrd_panel_q)
+        const bool queue = p.panel_nt == 0 && n > 512 && nb > sms && panel_smem<512, R>(n) <= 227 * 1024;
+        // otherwise one CTA per matrix: 256 threads (two CTAs per SM) for orders 385..512,
+        // 512 threads otherwise (measured), unless tuned
         bool mid = n > 384 && n <= 512;
-        if (n > 512) {
-            int dev = 0, sms = 148;
-            if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-                return RLMB_ERR_CUDA;
-            mid = nb > sms && nb <= 2 * sms && smem_of(256) <= 113 * 1024;
-        }
-        if (p.panel_nt == 256 && smem_of(256) <= 113 * 1024) mid = true;
+        if (p.panel_nt == 256 && panel_smem<256, R>(n) <= 113 * 1024) mid = true;
         if (p.panel_nt == 512) mid = false;
         auto panel = mid ? k_hetrd_panel<256, R> : k_hetrd_panel<512, R>;
         const int pnt = mid ? 256 : 512;
-        const size_t smem = smem_of(pnt);
-        if (cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        const size_t smem = mid ? panel_smem<256, R>(n) : panel_smem<512, R>(n);
+        if (cudaFuncSetAttribute(queue ? (const void*)k_hetrd_panel_q<512, R> : (const void*)panel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return RLMB_ERR_CUDA;
+        const int grid = std::min(nb, sms);
+        // the queue's counters, and its abort flag, which k_panel_abort_info reads in every case
+        if (cudaMemsetAsync(Q, 0, (8 + (size_t)nb) * sizeof(int), st) != cudaSuccess) return RLMB_ERR_CUDA;
         for (int k = 0; k < p.npanels; ++k) {
             RLMB_CHUNK_PROF("k_hetrd_panel");
-            panel<<<nb, pnt, smem, st>>>(A, D, E, TAU, PV, PWb, n, m);
+            if (queue)
+                k_hetrd_panel_q<512, R><<<grid, 512, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, nb, Q,
+                                                                 (long long)k * ((long long)nb * HP_W + grid),
+                                                                 k * HP_W, info);
+            else
+                panel<<<nb, pnt, smem, st>>>(A, D, E, TAU, PV, PWb, n, m);
             RLMB_CHUNK_LAUNCHED();
             m -= HP_W;
             RLMB_CHUNK_PROF("k_hetrd_her2k");
@@ -2244,6 +2351,13 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
     if (launch_hetrd<R>(p.hc, st, nb, A, D, E, TAU, n, m) != cudaSuccess) return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     return RLMB_OK;
+}
+
+// After the tridiagonal solve (which writes every matrix's info): a panel queue that ran out
+// of its bounded wait marks every matrix of the chunk as failed.
+__global__ void k_panel_abort_info(const int* __restrict__ Q, int* __restrict__ info, int nb) {
+    if (!*(volatile const int*)(Q + 1)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) info[i] = -1;
 }
 
 // Back-transformation X = Q Z in the working precision R (X column-major, column =
@@ -2397,8 +2511,10 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int 
     k_ref_diag<<<(unsigned)(((size_t)nb * n + 255) / 256), 256, 0, st>>>(ST, CL, W, F, n, nb);
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_update");
+    // X F is a correction of the size of the current error: FP32 sums over K (one drain per
+    // tile) carry it to well below the step's target
     if (launch_zgemm_tma<cplxf>(st, OpColA<cplx, XT>{X, n, nn}, OpColB<cplxf, cplxf>{F, n, nn},
-                                EpUpdate<XT>{X, Out, n}, n, n, n, nb, ctx->tws, ctx->tws_bytes) != cudaSuccess)
+                                EpUpdate<XT>{X, Out, n}, n, n, n, nb, ctx->tws, ctx->tws_bytes, false) != cudaSuccess)
         return RLMB_ERR_CUDA;
     RLMB_CHUNK_LAUNCHED();
     RLMB_CHUNK_PROF("k_ref_cluster");
@@ -2420,6 +2536,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     double* Ew = reinterpret_cast<double*>(base + p.off_e * B);
     double* Zw = reinterpret_cast<double*>(base + p.off_z * B);
     double* LUw = reinterpret_cast<double*>(base + p.off_lu * B);
+    int* Qw = reinterpret_cast<int*>(base + p.off_q * B);
     const size_t nn = (size_t)n * n;
     if (p.hc.smem > 227 * 1024 || p.smem_tri > 227 * 1024) return RLMB_ERR_ARG;
     if (cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_tri) != cudaSuccess ||
@@ -2431,7 +2548,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
         cplx* Tw = reinterpret_cast<cplx*>(base + p.off_t * B);
         cplx* Wp = reinterpret_cast<cplx*>(base + p.off_w * B);
         if (int rc = tridiagonalise<double>(ctx, st, p, nb, A, Dw, Ew, TAUw,
-                                            reinterpret_cast<cplx*>(base + p.off_pv * B), launches))
+                                            reinterpret_cast<cplx*>(base + p.off_pv * B), Qw, info, launches))
             return rc;
         RLMB_CHUNK_PROF("k_stebz");
         k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
@@ -2439,6 +2556,11 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
         RLMB_CHUNK_PROF("k_stein");
         k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
         RLMB_CHUNK_LAUNCHED();
+        if (info && p.npanels > 0) {
+            RLMB_CHUNK_PROF("k_stein");
+            k_panel_abort_info<<<(nb + 255) / 256, 256, 0, st>>>(Qw, info, nb);
+            RLMB_CHUNK_LAUNCHED();
+        }
         if (int rc = back_transform<double>(ctx, st, p, nb, A, TAUw, Zw, Xw, Tw, Wp, launches)) return rc;
         if (cudaMemcpyAsync(A, Xw, B * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
             return RLMB_ERR_CUDA;
@@ -2464,7 +2586,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     k_to_single<<<2048, 256, 0, st>>>(A, As, B * nn);
     RLMB_CHUNK_LAUNCHED();
     if (int rc = tridiagonalise<float>(ctx, st, p, nb, As, Dw, Ew, TAUw,
-                                       reinterpret_cast<cplxf*>(base + p.off_pv * B), launches))
+                                       reinterpret_cast<cplxf*>(base + p.off_pv * B), Qw, info, launches))
         return rc;
     RLMB_CHUNK_PROF("k_stebz");
     k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
@@ -2472,6 +2594,11 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     RLMB_CHUNK_PROF("k_stein");
     k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
     RLMB_CHUNK_LAUNCHED();
+    if (info && p.npanels > 0) {
+        RLMB_CHUNK_PROF("k_stein");
+        k_panel_abort_info<<<(nb + 255) / 256, 256, 0, st>>>(Qw, info, nb);
+        RLMB_CHUNK_LAUNCHED();
+    }
     if (int rc = back_transform<float>(ctx, st, p, nb, As, TAUw, Zw, Xw, Tw, Wp, launches)) return rc;
     // refinement, nb2 matrices at a time: the single-precision copy of H is free now and
     // holds F.  Step 1 starts from the single-precision vectors, step 2 from step 1's double

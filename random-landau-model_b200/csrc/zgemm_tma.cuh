@@ -22,8 +22,10 @@
 //     signalling a full mbarrier with the transaction byte count;
 //   * warp 9 (one thread) waits for the stage, issues its 12 MMAs (4 K steps x 3 products,
 //     M = N = 128) into one of two TMEM accumulators (256 columns), and frees the stage with
-//     tcgen05.commit; after every TMA_G blocks it commits the accumulator to the drain warps
-//     and switches to the other one (after the drain warps have released it);
+//     tcgen05.commit; after every G blocks it commits the accumulator to the drain warps and
+//     switches to the other one (after the drain warps have released it).  G = 1 sums every
+//     block's FP32 partial in double precision (error independent of K); G = all of K
+//     accumulates in FP32 in TMEM and drains once, leaving the tensor pipe unthrottled;
 //   * warps 0-7 (one TMEM lane quarter x 64 columns each) wait for each filled accumulator,
 //     read it with tcgen05.ld into FP32 registers, add it to 64 double-precision sums per
 //     thread, and release it; at the end they pair real and imaginary parts across lanes and
@@ -40,7 +42,8 @@ namespace rlmb {
 
 static constexpr int TMA_THREADS = 320;      // warps 0-7 drain, warp 8 loads, warp 9 issues MMAs
 static constexpr int TMA_STAGES = 3;
-static constexpr int TMA_G = 1;              // K blocks per accumulator drain
+static constexpr int TMA_G = 1;              // K blocks per accumulator drain (double-precision sums)
+static constexpr int TMA_G_ALL = 1 << 20;    // one drain at the end (FP32 accumulation)
 static constexpr int TMA_STAGE = 2 * TC_PLANE_A + 2 * TC_PLANE_B;   // both pieces of both operands
 static constexpr size_t TMA_SMEM = (size_t)TMA_STAGES * TMA_STAGE + 1024;
 static constexpr int TMA_KP = 32;            // K padding (complex) of the planes
@@ -142,7 +145,7 @@ k_tma_planes_b(LB lb, int N, int K, int Np, int Kp, size_t mat0, float* __restri
 }
 
 // ---------------------------------------------------------------- the GEMM
-template <class C, class EP>
+template <class C, class EP, int G = TMA_G>
 __global__ void __launch_bounds__(TMA_THREADS, 1)
 k_zgemm_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, EP ep, int M, int N,
             int Kp, int nbl, size_t mat0) {
@@ -185,7 +188,7 @@ k_zgemm_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
     const int nk = Kp / TC_KB;                   // K blocks
-    const int ng = (nk + TMA_G - 1) / TMA_G;     // accumulator groups
+    const int ng = (nk + G - 1) / G;             // accumulator groups
 
     if (warp == 8) {
         if (lane == 0) {   // ---- TMA producer
@@ -221,7 +224,7 @@ k_zgemm_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
                 }
                 const uint32_t acc = tmem + (uint32_t)(b * TC_BN);
                 bool ok = true;
-                for (int kb = g * TMA_G; kb < min(nk, (g + 1) * TMA_G); ++kb) {
+                for (int kb = g * G; kb < min(nk, (g + 1) * G); ++kb) {
                     const int s = kb % TMA_STAGES;
                     if (!tc_mbar_wait(&bar_full[s], (unsigned)((kb / TMA_STAGES) & 1))) {
                         ok = false;
@@ -234,7 +237,7 @@ k_zgemm_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
                     for (int j = 0; j < 4; ++j) {
                         const uint64_t ah = tc_desc(a + 32 * j), al = tc_desc(a + TC_PLANE_A + 32 * j);
                         const uint64_t bh = tc_desc(bb + 32 * j), bl = tc_desc(bb + TC_PLANE_B + 32 * j);
-                        tc_mma(acc, ah, bh, (kb != g * TMA_G || j != 0) ? 1u : 0u);
+                        tc_mma(acc, ah, bh, (kb != g * G || j != 0) ? 1u : 0u);
                         tc_mma(acc, ah, bl, 1);
                         tc_mma(acc, al, bh, 1);
                     }
@@ -333,10 +336,11 @@ inline size_t tma_plane_bytes(int M, int N, int K) {
 }
 
 // C = A B for nb matrices through planes in `ws` (ws_bytes, 256-byte aligned), in
-// sub-batches of as many matrices as the planes fit; returns a CUDA error.
+// sub-batches of as many matrices as the planes fit; the sums over K in double precision
+// (fp64_sum) or in FP32; returns a CUDA error.
 template <class C, class LA, class LB, class EP>
 cudaError_t launch_zgemm_tma(cudaStream_t st, const LA& la, const LB& lb, const EP& ep, int M, int N, int K, int nb,
-                             void* ws, size_t ws_bytes) {
+                             void* ws, size_t ws_bytes, bool fp64_sum = true) {
     if (M <= 0 || N <= 0 || nb <= 0) return cudaSuccess;
     if (K <= 0) return launch_zgemm_tc<C>(st, la, lb, ep, M, N, K, nb);   // zero product
     const int Mp = (M + TC_BM - 1) / TC_BM * TC_BM, Np = (N + TC_BN - 1) / TC_BN * TC_BN;
@@ -344,7 +348,7 @@ cudaError_t launch_zgemm_tma(cudaStream_t st, const LA& la, const LB& lb, const 
     const size_t per = tma_plane_bytes(M, N, K);
     const int sub = (int)std::min<size_t>((size_t)nb, ws_bytes / per);
     if (sub < 1 || !ws) return cudaErrorMemoryAllocation;
-    auto kern = k_zgemm_tma<C, EP>;
+    auto kern = fp64_sum ? k_zgemm_tma<C, EP, TMA_G> : k_zgemm_tma<C, EP, TMA_G_ALL>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TMA_SMEM);
     if (e != cudaSuccess) return e;
     for (int m0 = 0; m0 < nb; m0 += sub) {

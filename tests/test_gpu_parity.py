@@ -479,6 +479,46 @@ def test_heevd_back_transformation_blocks(n, bs, mixed):
         c.close()
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_panel_queue_matches_per_matrix_panels(mixed):
+    """A chunk of more matrices than SMs above order 512 runs its panels as one 512-thread CTA
+    per SM taking (matrix, column) units from a queue; it must give the results of the
+    one-CTA-per-matrix kernel of the same width (pinned with panel_threads = 512), and no
+    bounded wait may run out."""
+    import rlmb
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n, nb = 576, sms + 13
+    rng = np.random.default_rng(5)
+    a0 = rng.normal(size=(nb, n, n)) + 1j * rng.normal(size=(nb, n, n))
+    a0 = a0 + np.conj(np.transpose(a0, (0, 2, 1)))
+    out = []
+    for nt in (0, 512):
+        c = rlmb.Context(0)
+        try:
+            if mixed:
+                c.precision = c.MIXED
+            c.set_heev_config(n, 1, 1, nt, 0, 0)
+            a = torch.tensor(np.ascontiguousarray(np.transpose(a0, (0, 2, 1))), device="cuda")
+            info = torch.zeros(nb, dtype=torch.int32, device="cuda")
+            w = c.heevd(a, info=info)
+            torch.cuda.synchronize()
+            assert int(info.abs().sum()) == 0
+            assert c.tc_fault_count() == 0
+            out.append((w.cpu().numpy(), a.cpu().numpy()))
+        finally:
+            c.close()
+    (wq, xq), (wp, xp) = out
+    tol = 1e-10 if mixed else 1e-12
+    assert np.abs(wq - wp).max() <= tol * np.abs(wp).max()
+    for b in (0, nb // 2, nb - 1):
+        M = a0[b]
+        X = xq[b].T
+        wref = np.linalg.eigvalsh(M)
+        assert np.abs(wq[b] - wref).max() <= tol * np.abs(wref).max()
+        assert np.linalg.norm(M @ X - X * wq[b][None, :]) <= tol * np.linalg.norm(M)
+        assert np.linalg.norm(X.conj().T @ X - np.eye(n)) <= (1e-10 if mixed else 1e-11)
+
+
 def test_heevd_autotune_picks_and_caches():
     import rlmb
     c = rlmb.Context(0)
