@@ -70,12 +70,12 @@ int rlmb_get_precision(const rlmb_context* ctx);
 int rlmb_set_refinement_steps(rlmb_context* ctx, int steps);
 
 /* Eigensolver launch choices (no counterpart in the reference, whose solver is a library
- * call).  With autotuning on, the first eigensolve of each order n in 64..1024 and precision
+ * call).  With autotuning on, the first eigensolve of each order n in 16..1024 and precision
  * mode on the context times every feasible configuration -- unblocked or blocked reduction,
  * 256- or 512-thread panels, register-resident or GEMM back-transformation, 64- or
  * 128-reflector blocks and 64- or 128-row tiles of the double-precision X update of the
- * latter -- on copies of up to 2 x SMs of the call's own matrices and keeps the fastest for
- * later calls of that order.  rlmb_heev_config reports the configuration used for
+ * latter, and for n <= 80 the batched Jacobi solver -- on copies of up to 2 x SMs of the
+ * call's own matrices and keeps the fastest for later calls of that order.  rlmb_heev_config reports the configuration used for
  * (n, precision) (the tuned one, or the built-in one) and returns 1 if it was tuned or set,
  * 0 if built-in; rlmb_set_heev_config pins one (-1 / 0 = built-in choice for that item).
  * panel_threads, x_tile and bt_block 0 mean the built-in choice. */
@@ -84,6 +84,18 @@ int rlmb_heev_config(rlmb_context* ctx, int n, int precision, int* blocked, int*
                      int* x_tile, int* bt_block, double* ms_per_matrix);
 int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int blocked, int gemm_bt, int panel_threads,
                          int x_tile, int bt_block);
+/* Solver of the order-n eigensolves (no counterpart in the reference; both solvers stand in
+ * for its LAPACKE_zheevd call, diag_wrappers/mkl_diag.cpp:2-9).  RLMB_SOLVER_HOUSEHOLDER: the
+ * reduction / tridiagonal solve / back-transformation path above.  RLMB_SOLVER_JACOBI
+ * (n <= 80): two-sided cyclic Jacobi, one CTA per matrix with the matrix and its rotations in
+ * shared memory, double precision in either precision mode.  RLMB_SOLVER_AUTO: the built-in
+ * choice (Jacobi up to n = 20) or the autotuner's.  rlmb_heev_solver reports the solver that
+ * (n, precision) runs with now.  Jacobi above n = 80 returns RLMB_ERR_ARG. */
+#define RLMB_SOLVER_AUTO 0
+#define RLMB_SOLVER_HOUSEHOLDER 1
+#define RLMB_SOLVER_JACOBI 2
+int rlmb_set_heev_solver(rlmb_context* ctx, int n, int precision, int solver);
+int rlmb_heev_solver(rlmb_context* ctx, int n, int precision, int* solver);
 
 /* ------------------------------------------------- (b) Hermitian eigensolver
  * Batched full eigendecomposition, double precision, in place.

@@ -23,6 +23,7 @@
 //
 // Every wait is a __syncthreads inside one CTA: no inter-CTA dependencies, no spins.
 #include "common.cuh"
+#include "jacobi.cuh"
 #include "small_eig.cuh"
 #include "zgemm.cuh"
 #include "zgemm_tc.cuh"
@@ -1381,6 +1382,9 @@ struct EpSub {     // X(r, c) -= acc
 static constexpr int HP_W = 16;      // panel width (16 measured faster than 8, 12, 24 and 32 at orders 256-1000)
 static constexpr int HT_TAIL = 64;   // order below which the unblocked kernel finishes
 static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
+static constexpr int JAC_DEFAULT_MAX = 20;    // orders up to which k_jacobi is the built-in solver (measured: 2.1x the Householder path at 16, even at 24)
+static constexpr int TUNE_MIN_N = 16;         // orders the autotuner tunes: TUNE_MIN_N .. TUNE_MAX_N
+static constexpr int TUNE_MAX_N = 1024;
 
 // p += A v for the Hermitian leading m x m block stored in the upper triangle of a
 // (column-major, leading dimension ld; read only), v and p in shared memory.  Work is dealt
@@ -2187,6 +2191,7 @@ struct HeevTune {
     int panel_nt = 0;    // threads per panel CTA, 256 or 512
     int xtile = 0;       // row tile of the double-precision X -= V W' update, 64 or 128
     int bt_nb = 0;       // reflectors per block of the GEMM back-transformation, 64 or 128
+    int jacobi = -1;     // 1: batched Jacobi (k_jacobi, orders <= JAC_MAX_N), 0: the Householder path
 };
 
 // Shape of one eigensolve chunk: kernel configurations and the scratch layout per matrix
@@ -2194,6 +2199,8 @@ struct HeevTune {
 // starts aligned whatever the chunk size).
 struct HeevPlan {
     int n;
+    bool jacobi;         // k_jacobi in double precision (either mode); nothing below applies
+    size_t smem_jac;
     bool mixed;          // single-precision reduction + double refinement
     int refine_steps;    // mixed mode: 1 or 2
     int band;            // >= 0: every matrix is a cyclic band of this half-bandwidth (rlm), else -1
@@ -2221,6 +2228,12 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.mixed = mixed;
     p.band = band >= 0 && 32 + 2 * band <= n ? band : -1;   // the band residual needs 32 + 2o <= n
     p.refine_steps = mixed ? refine_steps : 0;
+    p.jacobi = n <= JAC_MAX_N && (tune.jacobi < 0 ? n <= JAC_DEFAULT_MAX : tune.jacobi > 0);
+    if (p.jacobi) {   // no scratch: the matrix and its rotations live in shared memory
+        p.smem_jac = jacobi_smem(n);
+        p.per = 256;
+        return p;
+    }
     const size_t ce = mixed ? sizeof(cplxf) : sizeof(cplx);   // working complex element
     const bool blocked = tune.blocked < 0 ? n >= HT_BLOCKED_MIN : (tune.blocked > 0 && n > HT_TAIL + HP_W);
     p.npanels = blocked ? (n - HT_TAIL + HP_W - 1) / HP_W : 0;
@@ -2538,6 +2551,15 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     double* LUw = reinterpret_cast<double*>(base + p.off_lu * B);
     int* Qw = reinterpret_cast<int*>(base + p.off_q * B);
     const size_t nn = (size_t)n * n;
+    if (p.jacobi) {
+        if (p.smem_jac > 227 * 1024) return RLMB_ERR_ARG;
+        if (cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_jac) != cudaSuccess)
+            return RLMB_ERR_CUDA;
+        RLMB_CHUNK_PROF("k_jacobi");
+        k_jacobi<<<nb, jacobi_threads(n), p.smem_jac, st>>>(A, W, info, n);
+        RLMB_CHUNK_LAUNCHED();
+        return RLMB_OK;
+    }
     if (p.hc.smem > 227 * 1024 || p.smem_tri > 227 * 1024) return RLMB_ERR_ARG;
     if (cudaFuncSetAttribute(k_tridiag<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_tri) != cudaSuccess ||
         cudaFuncSetAttribute(k_tridiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_tri) != cudaSuccess)
@@ -2641,9 +2663,10 @@ using namespace rlmb;
 // Per context, per (order, precision): the launch choices of HeevTune picked by timing every
 // feasible candidate -- unblocked or blocked reduction (from order 128), 256- or 512-thread
 // panels, register-resident or GEMM back-transformation, 64- or 128-reflector blocks and 64- or
-// 128-row X-update tiles (double precision) of the latter -- on copies of up to 2 x SMs of the call's own matrices (at most 2 GB of them),
-// each candidate run twice and timed the second time with CUDA events.  Orders 64 .. 1024
-// are tuned; others keep the built-in choices.
+// 128-row X-update tiles (double precision) of the latter, and up to order JAC_MAX_N the batched
+// Jacobi solver -- on copies of up to 2 x SMs of the call's own matrices (at most 2 GB of them),
+// each candidate run twice and timed the second time with CUDA events.  Orders
+// TUNE_MIN_N .. TUNE_MAX_N are tuned; others keep the built-in choices.
 struct TuneEntry {
     HeevTune t;
     double ms_per_matrix;
@@ -2660,6 +2683,11 @@ void rlmb::tune_free(rlmb_context* ctx) {
 
 static std::vector<HeevTune> tune_candidates(int n, bool mixed) {
     std::vector<HeevTune> out;
+    if (n <= JAC_MAX_N) {
+        HeevTune t;
+        t.jacobi = 1;
+        out.push_back(t);
+    }
     for (int blocked = 0; blocked <= 1; ++blocked) {
         if (blocked && n < 128) continue;
         for (int gemm = 0; gemm <= 1; ++gemm)
@@ -2670,6 +2698,7 @@ static std::vector<HeevTune> tune_candidates(int n, bool mixed) {
                         if ((!gemm || mixed) && xt == 128) continue;
                         if (!gemm && bs == 128) continue;
                         HeevTune t;
+                        t.jacobi = 0;
                         t.blocked = blocked;
                         t.gemm_bt = gemm;
                         t.panel_nt = blocked ? nt : 0;
@@ -2764,7 +2793,7 @@ int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n,
         auto it = tc.find({n, mixed ? 1 : 0});
         if (it != tc.end()) {
             tune = it->second.t;
-        } else if (ctx->autotune && !ctx->frozen && n >= 64 && n <= 1024) {
+        } else if (ctx->autotune && !ctx->frozen && n >= TUNE_MIN_N && n <= TUNE_MAX_N) {
             if (int rc = autotune(ctx, n, mixed, ctx->refine_steps, band, reinterpret_cast<const cplx*>(d_a), batch, &tune))
                 return rc;
         }
@@ -2847,13 +2876,41 @@ extern "C" int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int
         blocked > 1 || gemm_bt < -1 || gemm_bt > 1 || (panel_threads != 0 && panel_threads != 256 && panel_threads != 512) ||
         (x_tile != 0 && x_tile != 64 && x_tile != 128) || (bt_block != 0 && bt_block != 64 && bt_block != 128))
         return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
     HeevTune t;
+    if (it != tc.end()) t.jacobi = it->second.t.jacobi;   // the solver choice is set separately
     t.blocked = blocked;
     t.gemm_bt = gemm_bt;
     t.panel_nt = panel_threads;
     t.xtile = x_tile;
     t.bt_nb = bt_block;
-    tune_cache(ctx)[{n, precision}] = TuneEntry{t, 0.0};
+    tc[{n, precision}] = TuneEntry{t, 0.0};
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_set_heev_solver(rlmb_context* ctx, int n, int precision, int solver) {
+    if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED) ||
+        (solver != RLMB_SOLVER_AUTO && solver != RLMB_SOLVER_HOUSEHOLDER && solver != RLMB_SOLVER_JACOBI) ||
+        (solver == RLMB_SOLVER_JACOBI && n > JAC_MAX_N))
+        return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
+    TuneEntry e{HeevTune{}, 0.0};
+    if (it != tc.end()) e = it->second;
+    e.t.jacobi = solver == RLMB_SOLVER_AUTO ? -1 : solver == RLMB_SOLVER_JACOBI ? 1 : 0;
+    tc[{n, precision}] = e;
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_heev_solver(rlmb_context* ctx, int n, int precision, int* solver) {
+    if (!ctx || n <= 0 || !solver || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED))
+        return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
+    const HeevTune t = it != tc.end() ? it->second.t : HeevTune{};
+    *solver = heev_plan(n, precision == RLMB_PRECISION_MIXED, 2, -1, t).jacobi ? RLMB_SOLVER_JACOBI
+                                                                              : RLMB_SOLVER_HOUSEHOLDER;
     return RLMB_OK;
 }
 

@@ -41,6 +41,8 @@ _SIGNATURES = {
     "rlmb_heev_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip, _c_ip, _c_ip, _c_ip, _c_ip, _c_dp]),
     "rlmb_set_heev_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "rlmb_set_heev_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "rlmb_heev_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip]),
     "rlmb_zgemm_batched": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int]),
     "rlmb_tc_fault_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
@@ -269,6 +271,21 @@ class Context:
         prec = self.precision if precision is None else precision
         _check(lib().rlmb_set_heev_config(self.h, n, prec, blocked, gemm_bt, panel_threads, x_tile, bt_block),
                "rlmb_set_heev_config")
+
+    SOLVER_AUTO, SOLVER_HOUSEHOLDER, SOLVER_JACOBI = 0, 1, 2
+
+    def set_heev_solver(self, n, solver, precision=None):
+        """Pin the solver of order-n eigensolves: SOLVER_JACOBI (n <= 80), SOLVER_HOUSEHOLDER or
+        SOLVER_AUTO (built-in / autotuned)."""
+        prec = self.precision if precision is None else precision
+        _check(lib().rlmb_set_heev_solver(self.h, n, prec, solver), "rlmb_set_heev_solver")
+
+    def heev_solver(self, n, precision=None):
+        """SOLVER_JACOBI or SOLVER_HOUSEHOLDER: the solver order-n eigensolves run with now."""
+        prec = self.precision if precision is None else precision
+        v = ctypes.c_int()
+        _check(lib().rlmb_heev_solver(self.h, n, prec, ctypes.byref(v)), "rlmb_heev_solver")
+        return v.value
 
     GEMM_FP64, GEMM_TF32X3, GEMM_TF32X3_F64ACC = 0, 1, 2
 
