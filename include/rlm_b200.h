@@ -96,6 +96,19 @@ int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int blocked, i
 #define RLMB_SOLVER_JACOBI 2
 int rlmb_set_heev_solver(rlmb_context* ctx, int n, int precision, int solver);
 int rlmb_heev_solver(rlmb_context* ctx, int n, int precision, int* solver);
+/* Tridiagonal stage of the Householder solver (no counterpart in the reference; LAPACK's zheevd
+ * behind its LAPACKE_zheevd call solves this stage by divide and conquer).
+ * RLMB_TRIDIAG_BISECTION: eigenvalues by Sturm-count bisection, eigenvectors by twisted
+ * factorisation / inverse iteration.  RLMB_TRIDIAG_DC (n <= 3600): divide and conquer
+ * (Cuppen splits, deflation, secular equation per root, Gu-Eisenstat eigenvectors, merges as
+ * FP64 tensor-core GEMMs).  RLMB_TRIDIAG_AUTO: the built-in choice (divide and conquer from
+ * n = 600) or the autotuned one.  Both run in
+ * double precision in either precision mode. */
+#define RLMB_TRIDIAG_AUTO 0
+#define RLMB_TRIDIAG_BISECTION 1
+#define RLMB_TRIDIAG_DC 2
+int rlmb_set_tridiag_solver(rlmb_context* ctx, int n, int precision, int solver);
+int rlmb_tridiag_solver(rlmb_context* ctx, int n, int precision, int* solver);
 
 /* ------------------------------------------------- (b) Hermitian eigensolver
  * Batched full eigendecomposition, double precision, in place.

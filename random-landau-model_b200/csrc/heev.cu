@@ -24,6 +24,7 @@
 // Every wait is a __syncthreads inside one CTA: no inter-CTA dependencies, no spins.
 #include "common.cuh"
 #include "jacobi.cuh"
+#include "tridiag_dc.cuh"
 #include "small_eig.cuh"
 #include "zgemm.cuh"
 #include "zgemm_tc.cuh"
@@ -1382,6 +1383,7 @@ struct EpSub {     // X(r, c) -= acc
 static constexpr int HP_W = 16;      // panel width (16 measured faster than 8, 12, 24 and 32 at orders 256-1000)
 static constexpr int HT_TAIL = 64;   // order below which the unblocked kernel finishes
 static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
+static constexpr int DC_DEFAULT_MIN = 600;   // orders from which divide and conquer is the built-in tridiagonal solver (measured: even with bisection at 512, 1.4x at 1024, 2.3x at 3000)
 static constexpr int JAC_DEFAULT_MAX = 20;    // orders up to which k_jacobi is the built-in solver (measured: 2.1x the Householder path at 16, even at 24)
 static constexpr int TUNE_MIN_N = 16;         // orders the autotuner tunes: TUNE_MIN_N .. TUNE_MAX_N
 static constexpr int TUNE_MAX_N = 1024;
@@ -2192,6 +2194,8 @@ struct HeevTune {
     int xtile = 0;       // row tile of the double-precision X -= V W' update, 64 or 128
     int bt_nb = 0;       // reflectors per block of the GEMM back-transformation, 64 or 128
     int jacobi = -1;     // 1: batched Jacobi (k_jacobi, orders <= JAC_MAX_N), 0: the Householder path
+    int dc = -1;         // tridiagonal stage: 1 divide and conquer (orders <= DC_MAX_N), 0 bisection +
+                         // inverse iteration (k_tridiag)
 };
 
 // Shape of one eigensolve chunk: kernel configurations and the scratch layout per matrix
@@ -2201,6 +2205,8 @@ struct HeevPlan {
     int n;
     bool jacobi;         // k_jacobi in double precision (either mode); nothing below applies
     size_t smem_jac;
+    bool dc;             // divide-and-conquer tridiagonal stage (tridiag_dc.cuh) instead of k_tridiag
+    size_t off_q2, off_u, off_rot, off_sc;   // its second Q, U, rotations and scale
     bool mixed;          // single-precision reduction + double refinement
     int refine_steps;    // mixed mode: 1 or 2
     int band;            // >= 0: every matrix is a cyclic band of this half-bandwidth (rlm), else -1
@@ -2264,8 +2270,13 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.off_e = off; off += r256(n * sizeof(double));
     p.off_tau = off; off += r256(n * ce);
     p.off_a = off; off += mixed ? r256(nn * ce) : 0;        // single-precision copy of H, then F
+    p.dc = n <= DC_MAX_N && (tune.dc < 0 ? n >= DC_DEFAULT_MIN : tune.dc > 0);
     p.off_z = off; off += r256(nn * sizeof(double));
-    p.off_lu = off; off += r256(5 * (size_t)n * TRI_THREADS * sizeof(double));
+    p.off_lu = off; off += p.dc ? 0 : r256(5 * (size_t)n * TRI_THREADS * sizeof(double));
+    p.off_q2 = off; off += p.dc ? r256(nn * sizeof(double)) : 0;
+    p.off_u = off; off += p.dc ? r256(nn * sizeof(double)) : 0;
+    p.off_rot = off; off += p.dc ? r256((size_t)n * sizeof(DcRot)) : 0;
+    p.off_sc = off; off += p.dc ? 256 : 0;
     p.off_x = off; off += r256(nn * ce);
     p.off_t = off; off += r256((p.small_bt ? (size_t)p.nblk16 * ORM_NB * ORM_NB : (size_t)p.nblkbt * p.bt_nb * p.bt_nb) * ce);
     p.off_w = off; off += p.small_bt ? 0 : r256(2 * (size_t)p.bt_nb * n * ce);   // G and W' of a block
@@ -2284,13 +2295,21 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     return p;
 }
 
+// The allocation-free path's configuration: the built-in one with the bisection tridiagonal
+// solver, whose scratch sets its order limit.
+static HeevPlan noalloc_plan(int n) {
+    HeevTune t;
+    t.dc = 0;
+    return heev_plan(n, false, 2, -1, t);
+}
+
 // Bytes of scratch one matrix of order n needs in heev_chunk_on_scratch (double precision).
-size_t heev_scratch_bytes_per_matrix(int n) { return heev_plan(n, false).per; }
+size_t heev_scratch_bytes_per_matrix(int n) { return noalloc_plan(n).per; }
 
 // Largest chunk of matrices one heev_chunk call may take: the grid y / z extent (65535) of
 // the per-matrix launches, and of the (matrix, block) batches of the GEMM back-transformation.
 size_t heev_max_chunk(int n) {
-    const HeevPlan p = heev_plan(n, false);
+    const HeevPlan p = noalloc_plan(n);
     size_t c = 65535;
     if (!p.small_bt) c = std::min<size_t>(c, 65535 / std::max(p.nblkbt, 1));
     return c;
@@ -2540,6 +2559,61 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int 
 // per matrix as heev_plan describes (nb * plan.per bytes, no allocation).  Every scratch
 // region is written by a kernel before any kernel reads it.  ctx (optional) receives the
 // launch count and profile; otherwise *launches is advanced.
+// Eigenvalues W and eigenvectors Z (row-major) of the chunk's tridiagonals (D, E): bisection +
+// inverse iteration (k_tridiag), or divide and conquer level by level (k_dc_*), ending in Zw.
+static int tridiag_solve(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, int nb, unsigned char* base,
+                         const double* Dw, const double* Ew, double* W, double* Zw, double* LUw, int* info,
+                         long long* launches) {
+    const int n = p.n;
+    const size_t B = (size_t)nb;
+    if (!p.dc) {
+        RLMB_CHUNK_PROF("k_stebz");
+        k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+        RLMB_CHUNK_LAUNCHED();
+        RLMB_CHUNK_PROF("k_stein");
+        k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
+        RLMB_CHUNK_LAUNCHED();
+        return RLMB_OK;
+    }
+    double* Q2 = reinterpret_cast<double*>(base + p.off_q2 * B);
+    double* Uw = reinterpret_cast<double*>(base + p.off_u * B);
+    DcRot* Rw = reinterpret_cast<DcRot*>(base + p.off_rot * B);
+    double* SCw = reinterpret_cast<double*>(base + p.off_sc * B);
+    const int levels = dc_levels(n);
+    // ping-pong so that the last level writes Zw
+    double* qa = levels % 2 ? Q2 : Zw;
+    double* qb = levels % 2 ? Zw : Q2;
+    size_t smem_max = 0;   // (not monotone in S: small levels run 16 groups per CTA)
+    for (int S = 2; S / 2 < n; S *= 2) smem_max = std::max(smem_max, dc_smem(S, n));
+    if (smem_max > 227 * 1024) return RLMB_ERR_ARG;
+    if (cudaFuncSetAttribute(k_dc_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DgTiles)) !=
+            cudaSuccess)
+        return RLMB_ERR_CUDA;
+    RLMB_CHUNK_PROF("k_dc_merge");
+    k_dc_init<<<nb, 256, 0, st>>>(Dw, Ew, W, qa, SCw, info, n);
+    RLMB_CHUNK_LAUNCHED();
+    for (int S = 2; S / 2 < n; S *= 2) {
+        RLMB_CHUNK_PROF("k_dc_merge");
+        k_dc_merge<<<nb, DC_THREADS, dc_smem(S, n), st>>>(Ew, SCw, W, qa, qb, Uw, Rw, info, n, S);
+        RLMB_CHUNK_LAUNCHED();
+        if (S > DC_SMALL) {
+            const int nsub = (n + S - 1) / S;
+            const int mh = std::min(S / 2, n);
+            const dim3 grid((mh + DG_BM - 1) / DG_BM, (std::min(S, n) + DG_BN - 1) / DG_BN, nb * nsub * 2);
+            if (grid.z > 65535) return RLMB_ERR_ARG;
+            RLMB_CHUNK_PROF("k_dc_gemm");
+            k_dc_gemm<<<grid, 256, sizeof(DgTiles), st>>>(qa, Uw, qb, n, S, nsub);
+            RLMB_CHUNK_LAUNCHED();
+        }
+        std::swap(qa, qb);
+    }
+    RLMB_CHUNK_PROF("k_dc_merge");
+    k_dc_finish<<<std::min<size_t>(2048, (B * n + 255) / 256), 256, 0, st>>>(W, SCw, n, B * n);
+    RLMB_CHUNK_LAUNCHED();
+    return RLMB_OK;
+}
+
 static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cplx* A, double* W, int* info,
                       int nb, void* scratch, int nb2, long long* launches) {
     const int n = p.n;
@@ -2572,12 +2646,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
         if (int rc = tridiagonalise<double>(ctx, st, p, nb, A, Dw, Ew, TAUw,
                                             reinterpret_cast<cplx*>(base + p.off_pv * B), Qw, info, launches))
             return rc;
-        RLMB_CHUNK_PROF("k_stebz");
-        k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
-        RLMB_CHUNK_LAUNCHED();
-        RLMB_CHUNK_PROF("k_stein");
-        k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
-        RLMB_CHUNK_LAUNCHED();
+        if (int rc = tridiag_solve(ctx, st, p, nb, base, Dw, Ew, W, Zw, LUw, info, launches)) return rc;
         if (info && p.npanels > 0) {
             RLMB_CHUNK_PROF("k_stein");
             k_panel_abort_info<<<(nb + 255) / 256, 256, 0, st>>>(Qw, info, nb);
@@ -2610,12 +2679,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
     if (int rc = tridiagonalise<float>(ctx, st, p, nb, As, Dw, Ew, TAUw,
                                        reinterpret_cast<cplxf*>(base + p.off_pv * B), Qw, info, launches))
         return rc;
-    RLMB_CHUNK_PROF("k_stebz");
-    k_tridiag<1><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
-    RLMB_CHUNK_LAUNCHED();
-    RLMB_CHUNK_PROF("k_stein");
-    k_tridiag<2><<<nb, TRI_THREADS, p.smem_tri, st>>>(Dw, Ew, W, Zw, LUw, info, n);
-    RLMB_CHUNK_LAUNCHED();
+    if (int rc = tridiag_solve(ctx, st, p, nb, base, Dw, Ew, W, Zw, LUw, info, launches)) return rc;
     if (info && p.npanels > 0) {
         RLMB_CHUNK_PROF("k_stein");
         k_panel_abort_info<<<(nb + 255) / 256, 256, 0, st>>>(Qw, info, nb);
@@ -2652,7 +2716,7 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
 
 int heev_chunk_on_scratch(cudaStream_t st, cplx* A, double* W, int* info, int n, int nb, void* scratch,
                           long long* launches) {
-    return heev_chunk(nullptr, st, heev_plan(n, false), A, W, info, nb, scratch, 0, launches);
+    return heev_chunk(nullptr, st, noalloc_plan(n), A, W, info, nb, scratch, 0, launches);
 }
 
 }  // namespace rlmb
@@ -2663,8 +2727,8 @@ using namespace rlmb;
 // Per context, per (order, precision): the launch choices of HeevTune picked by timing every
 // feasible candidate -- unblocked or blocked reduction (from order 128), 256- or 512-thread
 // panels, register-resident or GEMM back-transformation, 64- or 128-reflector blocks and 64- or
-// 128-row X-update tiles (double precision) of the latter, and up to order JAC_MAX_N the batched
-// Jacobi solver -- on copies of up to 2 x SMs of the call's own matrices (at most 2 GB of them),
+// 128-row X-update tiles (double precision) of the latter, either tridiagonal solver (bisection +
+// inverse iteration, or divide and conquer), and up to order JAC_MAX_N the batched Jacobi solver -- on copies of up to 2 x SMs of the call's own matrices (at most 2 GB of them),
 // each candidate run twice and timed the second time with CUDA events.  Orders
 // TUNE_MIN_N .. TUNE_MAX_N are tuned; others keep the built-in choices.
 struct TuneEntry {
@@ -2706,7 +2770,10 @@ static std::vector<HeevTune> tune_candidates(int n, bool mixed) {
                         t.bt_nb = gemm ? bs : 0;
                         const HeevPlan p = heev_plan(n, mixed, 2, -1, t);
                         if (!gemm && !p.small_bt) continue;   // register back-transformation does not fit
-                        out.push_back(t);
+                        for (int dc = 0; dc <= (n <= DC_MAX_N ? 1 : 0); ++dc) {   // tridiagonal solver
+                            t.dc = dc;
+                            out.push_back(t);
+                        }
                     }
             }
     }
@@ -2819,6 +2886,7 @@ int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n,
     size_t chunk = std::max<size_t>(1, std::min<size_t>((budget - nb2 * per2) / per, (size_t)batch));
     chunk = std::min<size_t>(chunk, 65535);   // grid y / z extent of the per-matrix launches
     if (!plan.small_bt) chunk = std::min<size_t>(chunk, 65535 / std::max(plan.nblkbt, 1));   // (matrix, block) batches
+    if (plan.dc) chunk = std::min<size_t>(chunk, dc_max_chunk(n));   // (matrix, subproblem, half) GEMM batches
     // equal chunks: a short last chunk would leave most SMs idle in the one-CTA-per-matrix kernels
     const size_t nchunks = (batch + chunk - 1) / chunk;
     chunk = (batch + nchunks - 1) / nchunks;
@@ -2879,7 +2947,10 @@ extern "C" int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int
     auto& tc = tune_cache(ctx);
     auto it = tc.find({n, precision});
     HeevTune t;
-    if (it != tc.end()) t.jacobi = it->second.t.jacobi;   // the solver choice is set separately
+    if (it != tc.end()) {   // the solver choices are set separately
+        t.jacobi = it->second.t.jacobi;
+        t.dc = it->second.t.dc;
+    }
     t.blocked = blocked;
     t.gemm_bt = gemm_bt;
     t.panel_nt = panel_threads;
@@ -2900,6 +2971,30 @@ extern "C" int rlmb_set_heev_solver(rlmb_context* ctx, int n, int precision, int
     if (it != tc.end()) e = it->second;
     e.t.jacobi = solver == RLMB_SOLVER_AUTO ? -1 : solver == RLMB_SOLVER_JACOBI ? 1 : 0;
     tc[{n, precision}] = e;
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_set_tridiag_solver(rlmb_context* ctx, int n, int precision, int solver) {
+    if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED) ||
+        (solver != RLMB_TRIDIAG_AUTO && solver != RLMB_TRIDIAG_BISECTION && solver != RLMB_TRIDIAG_DC) ||
+        (solver == RLMB_TRIDIAG_DC && n > DC_MAX_N))
+        return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
+    TuneEntry e{HeevTune{}, 0.0};
+    if (it != tc.end()) e = it->second;
+    e.t.dc = solver == RLMB_TRIDIAG_AUTO ? -1 : solver == RLMB_TRIDIAG_DC ? 1 : 0;
+    tc[{n, precision}] = e;
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_tridiag_solver(rlmb_context* ctx, int n, int precision, int* solver) {
+    if (!ctx || n <= 0 || !solver || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED))
+        return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
+    const HeevTune t = it != tc.end() ? it->second.t : HeevTune{};
+    *solver = heev_plan(n, precision == RLMB_PRECISION_MIXED, 2, -1, t).dc ? RLMB_TRIDIAG_DC : RLMB_TRIDIAG_BISECTION;
     return RLMB_OK;
 }
 

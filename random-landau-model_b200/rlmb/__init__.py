@@ -43,6 +43,8 @@ _SIGNATURES = {
                                             ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "rlmb_set_heev_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "rlmb_heev_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip]),
+    "rlmb_set_tridiag_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "rlmb_tridiag_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip]),
     "rlmb_zgemm_batched": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int]),
     "rlmb_tc_fault_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
@@ -285,6 +287,21 @@ class Context:
         prec = self.precision if precision is None else precision
         v = ctypes.c_int()
         _check(lib().rlmb_heev_solver(self.h, n, prec, ctypes.byref(v)), "rlmb_heev_solver")
+        return v.value
+
+    TRIDIAG_AUTO, TRIDIAG_BISECTION, TRIDIAG_DC = 0, 1, 2
+
+    def set_tridiag_solver(self, n, solver, precision=None):
+        """Pin the tridiagonal stage of order-n eigensolves: TRIDIAG_DC (divide and conquer,
+        n <= 3600), TRIDIAG_BISECTION or TRIDIAG_AUTO (built-in / autotuned)."""
+        prec = self.precision if precision is None else precision
+        _check(lib().rlmb_set_tridiag_solver(self.h, n, prec, solver), "rlmb_set_tridiag_solver")
+
+    def tridiag_solver(self, n, precision=None):
+        """TRIDIAG_DC or TRIDIAG_BISECTION: the tridiagonal solver order-n eigensolves run with."""
+        prec = self.precision if precision is None else precision
+        v = ctypes.c_int()
+        _check(lib().rlmb_tridiag_solver(self.h, n, prec, ctypes.byref(v)), "rlmb_tridiag_solver")
         return v.value
 
     GEMM_FP64, GEMM_TF32X3, GEMM_TF32X3_F64ACC = 0, 1, 2
