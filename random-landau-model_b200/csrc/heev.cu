@@ -10,18 +10,23 @@
 //                  updates run as batched GEMMs over all SMs (launch_zgemm); the last leading
 //                  block (order <= 64, or all of a smaller matrix) by the unblocked,
 //                  look-ahead k_hetrd (zhetd2), its triangle resident in shared memory.
-//   tridiagonal    k_tridiag: eigenvalues by Sturm counts (dstebz restated, seeded from a
-//                  shared grid, Newton-accelerated); eigenvectors by twisted factorisation,
-//                  or for clusters inverse iteration / twisted solves with modified
-//                  Gram-Schmidt (dstein restated).
+//   tridiagonal    below order 600 k_tridiag: eigenvalues by Sturm counts (dstebz restated,
+//                  seeded from a shared grid, Newton-accelerated); eigenvectors by twisted
+//                  factorisation, or for clusters inverse iteration / twisted solves with
+//                  modified Gram-Schmidt (dstein restated).  From order 600 divide and
+//                  conquer (tridiag_dc.cuh: secular equations, Gu-Eisenstat vectors, DMMA
+//                  merges).  Either one may be pinned or autotuned per order.
 //   back-transform X = Q Z (zunmtr): k_larft + k_ormtr (register-resident Z chunks, blocks
 //                  of 16 reflectors) below order 256, else T factors from batched Gram
 //                  GEMMs and three GEMM launches per block of 64 reflectors.
 //   mixed mode     the reduction and back-transformation in single precision, then double
 //                  refinement of every eigenpair (k_ref_*, Ogita-Aishima restated, with
 //                  cluster Rayleigh-Ritz).
+//   small orders   up to order 20 (autotuned up to 80) the whole eigensolve is batched
+//                  two-sided Jacobi instead (jacobi.cuh).
 //
-// Every wait is a __syncthreads inside one CTA: no inter-CTA dependencies, no spins.
+// Waits are __syncthreads inside one CTA, except the panel queue's per-column counts
+// (k_hetrd_panel_q), whose spins are bounded in time and abort the chunk when they run out.
 #include "common.cuh"
 #include "jacobi.cuh"
 #include "tridiag_dc.cuh"
