@@ -925,7 +925,8 @@ def run_gpu_fss(args):
 
 def run_probe(args):
     """Small cases for profiler captures: --probe heevd runs one rlmb_heevd_batched call on
-    `batch` random Hermitian matrices of order n (--mixed: in the mixed mode); --probe tcgemm
+    `batch` random Hermitian matrices of order n (--mixed: in the mixed mode; --solver and
+    --tridiag pin the eigensolver and its tridiagonal stage); --probe tcgemm
     runs batched n x n x n complex GEMMs on the two tcgen05 engines (three each) and one on the
     DMMA engine, and prints their CUDA-event times; --probe rlm runs one rlm mesh solve of
     `batch` samples at order n, g=4."""
@@ -977,6 +978,10 @@ def run_probe(args):
         return
     if args.mixed:
         ctx.precision = ctx.MIXED
+    if args.solver != "auto":
+        ctx.set_heev_solver(n, ctx.SOLVER_JACOBI if args.solver == "jacobi" else ctx.SOLVER_HOUSEHOLDER)
+    if args.tridiag != "auto":
+        ctx.set_tridiag_solver(n, ctx.TRIDIAG_DC if args.tridiag == "dc" else ctx.TRIDIAG_BISECTION)
     a0 = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
     a = torch.tensor(np.ascontiguousarray(a0 + np.conj(np.transpose(a0, (0, 2, 1)))), device="cuda")
     ctx.heevd(a)
@@ -999,6 +1004,10 @@ def main():
     ap.add_argument("--mixed", action="store_true", help="probe in the mixed-precision mode")
     ap.add_argument("--probe", default=None, choices=["heevd", "tcgemm", "rlm", "hlm", "fhs"],
                     help="run one small eigensolver batch only (for profiler captures)")
+    ap.add_argument("--solver", default="auto", choices=["auto", "householder", "jacobi"],
+                    help="--probe heevd: pin the eigensolver of order n")
+    ap.add_argument("--tridiag", default="auto", choices=["auto", "bisection", "dc"],
+                    help="--probe heevd: pin the tridiagonal solver of order n")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=296)
     args = ap.parse_args()

@@ -48,9 +48,16 @@ struct DcRot {
     double c, s;   // rows (a, b) of U <- (c a - s b, s a + c b), applied in reverse order
 };
 
-__host__ __device__ inline int dc_group_threads(int S) {
-    const int g = ((S + 31) / 32) * 32;
-    return g < DC_THREADS ? g : DC_THREADS;
+// Threads per subproblem group: at least S (rounded to warps, at most DC_THREADS), and no more
+// groups than there are subproblems, so that every level keeps all DC_THREADS threads busy.
+// A power of two from 32 to DC_THREADS (at most 16 groups).
+__host__ __device__ inline int dc_group_threads(int S, int n) {
+    int g = ((S + 31) / 32) * 32;
+    g = g < DC_THREADS ? g : DC_THREADS;
+    const int nsub = (n + S - 1) / S;
+    int ng = DC_THREADS / g;
+    while (ng > 1 && ng > nsub) ng >>= 1;
+    return DC_THREADS / ng;
 }
 __host__ __device__ inline int dc_smax(int S, int n) { return S < n ? S : n; }
 __host__ __device__ inline size_t dc_group_bytes(int smax) {
@@ -58,7 +65,7 @@ __host__ __device__ inline size_t dc_group_bytes(int smax) {
     return 56 * m + 64;
 }
 __host__ __device__ inline size_t dc_smem(int S, int n) {
-    return (size_t)(DC_THREADS / dc_group_threads(S)) * dc_group_bytes(dc_smax(S, n));
+    return (size_t)(DC_THREADS / dc_group_threads(S, n)) * dc_group_bytes(dc_smax(S, n));
 }
 // number of merge levels: S = 2, 4, ... while S / 2 < n
 __host__ __device__ inline int dc_levels(int n) {
@@ -139,7 +146,38 @@ __device__ __forceinline__ int dc_upper(const double* v, int m, double x) {
     return lo;
 }
 
-// One level of merges: one CTA of DC_THREADS per matrix, a group of dc_group_threads(S)
+// Pole sums of the secular function over k in [k0, k1): sw = sum w_k and sw2 = sum w_k / delta_k
+// with w_k = z_k^2 / delta_k, delta_k = (d_k - d0) - t.  Four independent accumulator pairs,
+// so that four reciprocals are in flight at once.
+__device__ __forceinline__ void dc_pole_sums(const double* __restrict__ ds, const double* __restrict__ zs, int k0,
+                                             int k1, double d0, double t, double& sw, double& sw2) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+    int k = k0;
+    for (; k + 3 < k1; k += 4) {
+        const double r0 = 1.0 / ((ds[k] - d0) - t), r1 = 1.0 / ((ds[k + 1] - d0) - t);
+        const double r2 = 1.0 / ((ds[k + 2] - d0) - t), r3 = 1.0 / ((ds[k + 3] - d0) - t);
+        const double w0 = zs[k] * zs[k] * r0, w1 = zs[k + 1] * zs[k + 1] * r1;
+        const double w2 = zs[k + 2] * zs[k + 2] * r2, w3 = zs[k + 3] * zs[k + 3] * r3;
+        a0 += w0;
+        a1 += w1;
+        a2 += w2;
+        a3 += w3;
+        b0 = fma(w0, r0, b0);
+        b1 = fma(w1, r1, b1);
+        b2 = fma(w2, r2, b2);
+        b3 = fma(w3, r3, b3);
+    }
+    for (; k < k1; ++k) {
+        const double r = 1.0 / ((ds[k] - d0) - t);
+        const double w = zs[k] * zs[k] * r;
+        a0 += w;
+        b0 = fma(w, r, b0);
+    }
+    sw = (a0 + a1) + (a2 + a3);
+    sw2 = (b0 + b1) + (b2 + b3);
+}
+
+// One level of merges: one CTA of DC_THREADS per matrix, a group of dc_group_threads(S, n)
 // threads per subproblem of size S (children S/2 and the rest).  W holds the children's
 // sorted eigenvalues on entry and the merged ones on return; Qo the children's eigenvectors,
 // Qn the merged ones (for S <= DC_SMALL, else U for k_dc_gemm).
@@ -148,7 +186,7 @@ k_dc_merge(const double* __restrict__ E, const double* __restrict__ SC, double* 
            const double* __restrict__ Qo, double* __restrict__ Qn, double* __restrict__ U, DcRot* __restrict__ ROT,
            int* __restrict__ info, int n, int S) {
     extern __shared__ __align__(16) unsigned char dc_sm[];
-    const int gs = dc_group_threads(S), ng = DC_THREADS / gs;
+    const int gs = dc_group_threads(S, n), ng = DC_THREADS / gs;
     const int grp = threadIdx.x / gs, gt = threadIdx.x % gs;
     const int smax = dc_smax(S, n);
     const int sm8 = (smax + 7) / 8 * 8;
@@ -268,11 +306,9 @@ k_dc_merge(const double* __restrict__ E, const double* __restrict__ SC, double* 
             if (j < K - 1) {
                 const double dj = ds[j];
                 const double mid = 0.5 * (ds[j + 1] - dj);
-                double f = rrho;
-                for (int k = 0; k < K; ++k) {
-                    const double zk = zs[k];
-                    f += zk * zk / ((ds[k] - dj) - mid);
-                }
+                double fs, fd;
+                dc_pole_sums(ds, zs, 0, K, dj, mid, fs, fd);
+                const double f = rrho + fs;
                 if (f >= 0.0) {
                     og = j;
                     lo = 0.0;
@@ -293,19 +329,9 @@ k_dc_merge(const double* __restrict__ E, const double* __restrict__ SC, double* 
             double t = 0.5 * (lo + hi);
             bool conv = false;
             for (int it = 0; it < DC_MAX_ITS; ++it) {
-                double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
-                for (int k = 0; k <= j; ++k) {
-                    const double r = 1.0 / ((ds[k] - d0) - t);
-                    const double w = zs[k] * zs[k] * r;
-                    psi += w;
-                    dpsi += w * r;
-                }
-                for (int k = j + 1; k < K; ++k) {
-                    const double r = 1.0 / ((ds[k] - d0) - t);
-                    const double w = zs[k] * zs[k] * r;
-                    phi += w;
-                    dphi += w * r;
-                }
+                double psi, dpsi, phi, dphi;
+                dc_pole_sums(ds, zs, 0, j + 1, d0, t, psi, dpsi);
+                dc_pole_sums(ds, zs, j + 1, K, d0, t, phi, dphi);
                 const double f = rrho + psi + phi;
                 if (f < 0.0) lo = t;
                 else hi = t;
@@ -360,12 +386,15 @@ k_dc_merge(const double* __restrict__ E, const double* __restrict__ SC, double* 
         // z from the roots (Gu & Eisenstat): pairs (x_j - d_i) / (d_j - d_i), and (x_i - d_i) / rho
         for (int i = gt; i < K; i += gs) {
             const double di = ds[i];
-            double p = 1.0;
-            for (int j = 0; j < K; ++j) {
-                const double xmd = (ds[org[j]] - di) + tau[j];
-                p *= xmd / (j == i ? rho : ds[j] - di);
+            double p0 = 1.0, p1 = 1.0;   // even and odd j: two divisions in flight
+            int j = 0;
+            for (; j + 1 < K; j += 2) {
+                const double x0 = (ds[org[j]] - di) + tau[j], x1 = (ds[org[j + 1]] - di) + tau[j + 1];
+                p0 *= x0 / (j == i ? rho : ds[j] - di);
+                p1 *= x1 / (j + 1 == i ? rho : ds[j + 1] - di);
             }
-            zh[i] = copysign(sqrt(fmax(p, 0.0)), zs[i]);
+            if (j < K) p0 *= ((ds[org[j]] - di) + tau[j]) / (j == i ? rho : ds[j] - di);
+            zh[i] = copysign(sqrt(fmax(p0 * p1, 0.0)), zs[i]);
         }
         for (int j = gt; j < K; j += gs) vals[j] = ds[org[j]] + tau[j];
         dc_sync(grp, gs);
@@ -386,13 +415,21 @@ k_dc_merge(const double* __restrict__ E, const double* __restrict__ SC, double* 
             const int col = pos[c];
             if (c < K) {
                 const double x0 = ds[org[c]], tc = tau[c];
-                double nrm = 0.0;
-                for (int i = 0; i < K; ++i) {
-                    const double dl = (ds[i] - x0) - tc;
-                    const double u = zh[i] / dl;
-                    nrm += u * u;
+                double n0 = 0.0, n1 = 0.0, n2 = 0.0, n3 = 0.0;
+                int i = 0;
+                for (; i + 3 < K; i += 4) {
+                    const double u0 = zh[i] / ((ds[i] - x0) - tc), u1 = zh[i + 1] / ((ds[i + 1] - x0) - tc);
+                    const double u2 = zh[i + 2] / ((ds[i + 2] - x0) - tc), u3 = zh[i + 3] / ((ds[i + 3] - x0) - tc);
+                    n0 = fma(u0, u0, n0);
+                    n1 = fma(u1, u1, n1);
+                    n2 = fma(u2, u2, n2);
+                    n3 = fma(u3, u3, n3);
                 }
-                const double rn = 1.0 / sqrt(nrm);
+                for (; i < K; ++i) {
+                    const double u = zh[i] / ((ds[i] - x0) - tc);
+                    n0 = fma(u, u, n0);
+                }
+                const double rn = 1.0 / sqrt((n0 + n1) + (n2 + n3));
                 for (int i = 0; i < K; ++i) {
                     const double dl = (ds[i] - x0) - tc;
                     us[(size_t)perm[src[i]] * K0 + col] = zh[i] / dl * rn;
