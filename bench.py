@@ -15,7 +15,11 @@ value : FP64 mode, rlmb_rlm_mesh_solve_device per step (results stay in device m
 e2e   : the host-buffer C-ABI call rlmb_rlm_mesh_solve (coefficient tables H2D, energies and
         Chern numbers D2H inside the timed region), FP64 mode.
 mixed : the mixed-precision mode (tcgen05 tensor-core products, FP64 refinement) on the same
-        samples, with its agreement with the FP64 mode and with the reference fixture.
+        samples, with its agreement with the FP64 mode and with the reference fixture, in two
+        variants: one refinement step + the Rayleigh-quotient eigenvalue pass, and two steps.
+        The headline mixed figure is the faster variant that meets the accuracy target in
+        this run (energies within 1e-10 of the FP64 mode and of the fixture, Chern integers
+        identical); the other is nested in it.
 extra : the hlm 48x16 configuration (n_phi = 256, g = 32, 64 samples per step).
 --impl reference : the reference's own CPU implementation (oracle/_ref, compiled from the
         reference sources) on this host's cores, one k-point per step.
@@ -707,18 +711,19 @@ def run_headline(args):
     ev1.record()
     barrier()
     ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))
-    # ---- mixed mode on the same samples
-    m_steps = max(1, min(args.steps, 5))
+    # ---- mixed mode on the same samples: one refinement step + the Rayleigh-quotient
+    #      eigenvalue pass (the accuracy the energies and Chern numbers need) ...
+    mq_steps = max(1, min(args.steps, 5))
+    ctx.set_refinement_steps(1)
+    ctx.set_eigenvalue_pass(True)
+    ms_rq, prof_rq, _, _ = timed("mixed", mq_steps, 3)
+    erq, crq = d_e.cpu().numpy(), d_c.cpu().numpy()
+    ctx.set_eigenvalue_pass(False)
+    ctx.set_refinement_steps(2)
+    # ---- ... and two refinement steps (double-precision eigenvectors as well)
+    m_steps = max(1, min(args.steps, 3))
     ms_mix, prof_mix, _, _ = timed("mixed", m_steps, 3)
     em, cm = d_e.cpu().numpy(), d_c.cpu().numpy()
-    # ---- mixed mode with one refinement step (the accuracy the Chern numbers need)
-    ms_mix1 = None
-    if not args.no_extra:
-        m1_steps = max(1, min(args.steps, 3))
-        ctx.set_refinement_steps(1)
-        ms_mix1, prof_mix1, _, _ = timed("mixed", m1_steps, 3)
-        em1, cm1 = d_e.cpu().numpy(), d_c.cpu().numpy()
-        ctx.set_refinement_steps(2)
     ctx.precision = ctx.FP64
     faults = ctx.tc_fault_count()
     extra = _hlm_extra(ctx) if (ws == 1 and not args.no_extra) else None
@@ -726,6 +731,7 @@ def run_headline(args):
     value = ws * solves * args.steps / (ms_dev * 1e-3)
     e2e = ws * solves * e2e_steps / (ms_e2e * 1e-3)
     v_mix = ws * solves * m_steps / (ms_mix * 1e-3)
+    v_rq = ws * solves * mq_steps / (ms_rq * 1e-3)
     line = None
     if rank == 0:
         peaks = _measured_peaks()
@@ -738,7 +744,8 @@ def run_headline(args):
             fx = np.load(RLM_FIXTURE)
             eref, cref = fx["energies"][0], fx["chern"][0]
             par = {"fixture": os.path.relpath(RLM_FIXTURE, REPO), "sample": 0}
-            for mode, (e, c) in (("fp64", (e64, c64)), ("mixed", (em, cm))):
+            for mode, (e, c) in (("fp64", (e64, c64)), ("mixed_one_step_rq", (erq, crq)),
+                                 ("mixed_two_steps", (em, cm))):
                 par[mode] = {"max_energy_rel_error": float(np.abs(e[0] - eref).max() / np.abs(eref).max()),
                              "chern_integers_identical": bool(np.array_equal(np.rint(c[0]), np.rint(cref))),
                              "max_chern_deviation": float(np.abs(c[0] - cref).max())}
@@ -791,24 +798,35 @@ def run_headline(args):
                 tc[k] = {"achieved_tf32_tflops": tf, "useful_complex_tflops": tf / 3.0, "peak_tf32_tflops": tf32_peak,
                          "frac": tf / tf32_peak,
                          "peak_source": f"{bf16_src} bf16 dense / 2 (TF32 runs at half the BF16 rate)"}
-        mixed = {"value": v_mix, "unit": UNIT, "ms_per_step": ms_mix / m_steps, "steps": m_steps, "warmup": 3,
-                 "samples_per_hour": v_mix / RLM_KPTS * 3600.0,
-                 "samples_per_hour_ratio_to_fp64": v_mix / value,
-                 "refinement_steps": 2,
-                 "chern_integers_identical_to_fp64": bool(np.array_equal(np.rint(cm), np.rint(c64))),
-                 "max_chern_deviation_from_fp64": float(np.abs(cm - c64).max()),
-                 "max_energy_rel_error_vs_fp64": float(np.abs(em - e64).max() / np.abs(e64).max()),
-                 "tensor_core_roofline": tc, "tc_faults": faults,
-                 "kernel_ms_per_step": {k: v[0] / m_steps for k, v in sorted(prof_mix.items())}}
-        if ms_mix1 is not None:
-            v1 = ws * solves * m1_steps / (ms_mix1 * 1e-3)
-            mixed["one_refinement_step"] = {
-                "value": v1, "unit": UNIT, "ms_per_step": ms_mix1 / m1_steps, "steps": m1_steps, "warmup": 3,
-                "samples_per_hour_ratio_to_fp64": v1 / value,
-                "chern_integers_identical_to_fp64": bool(np.array_equal(np.rint(cm1), np.rint(c64))),
-                "max_chern_deviation_from_fp64": float(np.abs(cm1 - c64).max()),
-                "max_energy_rel_error_vs_fp64": float(np.abs(em1 - e64).max() / np.abs(e64).max()),
-                "kernel_ms_per_step": {k: v[0] / m1_steps for k, v in sorted(prof_mix1.items())}}
+        def variant(v, ms, steps, e, c, prf, refinement):
+            rec = {"value": v, "unit": UNIT, "ms_per_step": ms / steps, "steps": steps, "warmup": 3,
+                   "samples_per_hour": v / RLM_KPTS * 3600.0,
+                   "samples_per_hour_ratio_to_fp64": v / value,
+                   "refinement": refinement,
+                   "chern_integers_identical_to_fp64": bool(np.array_equal(np.rint(c), np.rint(c64))),
+                   "max_chern_deviation_from_fp64": float(np.abs(c - c64).max()),
+                   "max_energy_rel_error_vs_fp64": float(np.abs(e - e64).max() / np.abs(e64).max()),
+                   "kernel_ms_per_step": {k: x[0] / steps for k, x in sorted(prf.items())}}
+            # the north star's accuracy target, checked on this run's timed samples (against the
+            # FP64 mode) and on sample 0 (against the reference's fixture)
+            ok = rec["chern_integers_identical_to_fp64"] and rec["max_energy_rel_error_vs_fp64"] <= 1e-10
+            return rec, ok
+        rq, rq_ok = variant(v_rq, ms_rq, mq_steps, erq, crq, prof_rq,
+                            "1 step + Rayleigh-quotient eigenvalues (rlmb_set_eigenvalue_pass)")
+        two, two_ok = variant(v_mix, ms_mix, m_steps, em, cm, prof_mix, "2 steps")
+        two["tensor_core_roofline"] = tc
+        if par:
+            rq_ok = rq_ok and par["mixed_one_step_rq"]["max_energy_rel_error"] <= 1e-10 and \
+                par["mixed_one_step_rq"]["chern_integers_identical"]
+            two_ok = two_ok and par["mixed_two_steps"]["max_energy_rel_error"] <= 1e-10 and \
+                par["mixed_two_steps"]["chern_integers_identical"]
+        rq["meets_accuracy_target"], two["meets_accuracy_target"] = rq_ok, two_ok
+        # headline mixed figure: the faster variant that meets the accuracy target
+        if rq_ok and v_rq >= v_mix:
+            mixed = dict(rq, two_refinement_steps=two)
+        else:
+            mixed = dict(two, one_refinement_step_rq=rq)
+        mixed["tc_faults"] = faults
         nb = 2 * 221 * 221 + 2 * (g + 1) * 221 + 2 * n * 221   # coefficient tables (complex) ...
         h2d = 8 * nb + 2 * RLM_KPTS * ns * 4                    # ... + the theta lists
         line = {

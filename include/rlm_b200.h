@@ -68,6 +68,14 @@ int rlmb_get_precision(const rlmb_context* ctx);
  * orthogonality defects of ~1e-12..1e-7 (growing with n), two reach double-precision
  * level.  Eigenvalues are within ~1e-11 relative after one step. */
 int rlmb_set_refinement_steps(rlmb_context* ctx, int steps);
+/* Mixed mode with one refinement step only (no counterpart in the reference): with the pass on,
+ * every eigenvalue is recomputed after the step as the Rayleigh quotient of its refined vector,
+ * x^H H x / x^H x, from a double-precision residual R = H X - X diag(w) (banded for the rlm
+ * meshes).  The quotient's error is of the order of the square of the vector's (~1e-7 after
+ * one step), so the eigenvalues reach double-precision level at the cost of one residual
+ * instead of a second full step; the eigenvectors keep the one-step accuracy (residual and
+ * orthogonality ~1e-7).  Off by default; no effect with two steps or in the FP64 mode. */
+int rlmb_set_eigenvalue_pass(rlmb_context* ctx, int on);
 
 /* Eigensolver launch choices (no counterpart in the reference, whose solver is a library
  * call).  With autotuning on, the first eigensolve of each order n in 16..1024 and precision

@@ -224,6 +224,12 @@ int rlmb_set_refinement_steps(rlmb_context* ctx, int steps) {
     return RLMB_OK;
 }
 
+int rlmb_set_eigenvalue_pass(rlmb_context* ctx, int on) {
+    if (!ctx) return RLMB_ERR_ARG;
+    ctx->rq_pass = on ? 1 : 0;
+    return RLMB_OK;
+}
+
 const char* rlmb_status_string(int status) {
     switch (status) {
         case RLMB_OK: return "ok";

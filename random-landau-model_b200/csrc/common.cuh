@@ -147,6 +147,9 @@ struct rlmb_context {
     // steps (rlmb_set_precision, rlmb_set_refinement_steps)
     int precision;
     int refine_steps;
+    // mixed mode, one refinement step: recompute every eigenvalue afterwards as the Rayleigh
+    // quotient of its refined vector (rlmb_set_eigenvalue_pass)
+    int rq_pass;
 };
 
 #define RLMB_CUDA_TRY(expr)                                                       \

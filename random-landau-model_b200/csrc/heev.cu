@@ -2214,6 +2214,7 @@ struct HeevPlan {
     size_t off_q2, off_u, off_rot, off_sc;   // its second Q, U, rotations and scale
     bool mixed;          // single-precision reduction + double refinement
     int refine_steps;    // mixed mode: 1 or 2
+    bool rq;             // mixed mode, one step: then the eigenvalues as Rayleigh quotients (H kept until then)
     int band;            // >= 0: every matrix is a cyclic band of this half-bandwidth (rlm), else -1
     HetrdCfg hc;
     size_t smem_tri;
@@ -2238,7 +2239,9 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.n = n;
     p.mixed = mixed;
     p.band = band >= 0 && 32 + 2 * band <= n ? band : -1;   // the band residual needs 32 + 2o <= n
-    p.refine_steps = mixed ? refine_steps : 0;
+    // refine_steps 3 (heev_steps): one step, then the Rayleigh-quotient eigenvalue pass
+    p.rq = mixed && refine_steps == 3;
+    p.refine_steps = mixed ? (refine_steps == 3 ? 1 : refine_steps) : 0;
     p.jacobi = n <= JAC_MAX_N && (tune.jacobi < 0 ? n <= JAC_DEFAULT_MAX : tune.jacobi > 0);
     if (p.jacobi) {   // no scratch: the matrix and its rotations live in shared memory
         p.smem_jac = jacobi_smem(n);
@@ -2296,7 +2299,7 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.per = off;
     p.per2 = mixed ? r256(nn * sizeof(cplx)) : 0;                              // residual R
     p.off2_x1 = p.per2;
-    p.per2 += p.refine_steps >= 2 ? r256(nn * sizeof(cplx)) : 0;                 // step-1 vectors
+    p.per2 += p.refine_steps >= 2 || p.rq ? r256(nn * sizeof(cplx)) : 0;         // step-1 vectors
     return p;
 }
 
@@ -2560,10 +2563,35 @@ static int refine_step(rlmb_context* ctx, cudaStream_t st, int n, int band, int 
     return RLMB_OK;
 }
 
-// The kernel sequence of one eigensolve chunk of nb matrices of order n on scratch laid out
-// per matrix as heev_plan describes (nb * plan.per bytes, no allocation).  Every scratch
-// region is written by a kernel before any kernel reads it.  ctx (optional) receives the
-// launch count and profile; otherwise *launches is advanced.
+// w_j <- w_j + Re(x_j^H r_j) / x_j^H x_j for every column: the Rayleigh quotient of x_j, r = H x - x w.
+__global__ void k_ref_rq(const double* __restrict__ ST, double* __restrict__ W, size_t total) {
+    const size_t gj = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gj < total) W[gj] += ST[3 * gj + 1] / ST[3 * gj];
+}
+
+// The eigenvalue pass after one refinement step: residual of the refined double-precision
+// vectors X against H (banded for the rlm meshes), column statistics, Rayleigh quotients.
+static int rayleigh_pass(cudaStream_t st, int n, int band, int nb, const cplx* A, const cplx* X, double* W,
+                         cplx* Res, double* ST, rlmb_context* ctx, long long* launches) {
+    const size_t nn = (size_t)n * n;
+    const unsigned gw = (unsigned)(((size_t)nb * n + 7) / 8);
+    RLMB_CHUNK_PROF("k_ref_resid");
+    if (band >= 0) {
+        k_ref_resid_band<cplx><<<dim3((n + 31) / 32, (n + 63) / 64, nb), 256, 0, st>>>(A, X, W, Res, n, band);
+    } else if (launch_zgemm<cplx, 64>(st, OpColA<cplx, cplx>{A, n, nn}, OpColB<cplx, cplx>{X, n, nn},
+                                      EpResid<cplx>{X, W, Res, n}, n, n, n, nb) != cudaSuccess) {
+        return RLMB_ERR_CUDA;
+    }
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_colstats");
+    k_ref_colstats<cplx><<<gw, 256, 0, st>>>(X, Res, ST, n, nb);
+    RLMB_CHUNK_LAUNCHED();
+    RLMB_CHUNK_PROF("k_ref_diag");
+    k_ref_rq<<<(unsigned)(((size_t)nb * n + 255) / 256), 256, 0, st>>>(ST, W, (size_t)nb * n);
+    RLMB_CHUNK_LAUNCHED();
+    return RLMB_OK;
+}
+
 // Eigenvalues W and eigenvectors Z (row-major) of the chunk's tridiagonals (D, E): bisection +
 // inverse iteration (k_tridiag), or divide and conquer level by level (k_dc_*), ending in Zw.
 static int tridiag_solve(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, int nb, unsigned char* base,
@@ -2619,6 +2647,10 @@ static int tridiag_solve(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, 
     return RLMB_OK;
 }
 
+// The kernel sequence of one eigensolve chunk of nb matrices of order n on scratch laid out
+// per matrix as heev_plan describes (nb * plan.per bytes, no allocation).  Every scratch
+// region is written by a kernel before any kernel reads it.  ctx (optional) receives the
+// launch count and profile; otherwise *launches is advanced.
 static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cplx* A, double* W, int* info,
                       int nb, void* scratch, int nb2, long long* launches) {
     const int n = p.n;
@@ -2707,8 +2739,13 @@ static int heev_chunk(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, cpl
         double* MUm = MU + on;
         double* STm = ST + 3 * on;
         if (int rc = refine_step<cplxf>(ctx, st, n, p.band, ns, Am, Xw + o, Wm, Res, Fm, CLm, YBm, MUm, STm,
-                                        p.refine_steps >= 2 ? X1 : Am, launches))
+                                        p.refine_steps >= 2 || p.rq ? X1 : Am, launches))
             return rc;
+        if (p.rq) {   // eigenvalues as Rayleigh quotients of the step-1 vectors, then the vectors out
+            if (int rc = rayleigh_pass(st, n, p.band, ns, Am, X1, Wm, Res, STm, ctx, launches)) return rc;
+            if (cudaMemcpyAsync(Am, X1, (size_t)ns * nn * sizeof(cplx), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+                return RLMB_ERR_CUDA;
+        }
         if (p.refine_steps >= 2)
             if (int rc = refine_step<cplx>(ctx, st, n, p.band, ns, Am, X1, Wm, Res, Fm, CLm, YBm, MUm, STm, Am,
                                            launches))
@@ -2851,6 +2888,9 @@ static int autotune(rlmb_context* ctx, int n, bool mixed, int refine_steps, int 
     return rc;
 }
 
+// Refinement steps handed to heev_plan: 1 or 2, or 3 for one step followed by the eigenvalue pass.
+static int heev_steps(const rlmb_context* ctx) { return ctx->refine_steps == 1 && ctx->rq_pass ? 3 : ctx->refine_steps; }
+
 // The batched eigensolve of rlmb_heevd_batched with a structure hint: band >= 0 declares every
 // matrix a cyclic band of that half-bandwidth (the rlm Hamiltonian), which the mixed mode's
 // refinement uses for its residual; band < 0 is a dense matrix.
@@ -2866,11 +2906,11 @@ int rlmb::heevd_batched_band(rlmb_context* ctx, double* d_a, double* d_w, int n,
         if (it != tc.end()) {
             tune = it->second.t;
         } else if (ctx->autotune && !ctx->frozen && n >= TUNE_MIN_N && n <= TUNE_MAX_N) {
-            if (int rc = autotune(ctx, n, mixed, ctx->refine_steps, band, reinterpret_cast<const cplx*>(d_a), batch, &tune))
+            if (int rc = autotune(ctx, n, mixed, heev_steps(ctx), band, reinterpret_cast<const cplx*>(d_a), batch, &tune))
                 return rc;
         }
     }
-    const HeevPlan plan = heev_plan(n, mixed, ctx->refine_steps, band, tune);
+    const HeevPlan plan = heev_plan(n, mixed, heev_steps(ctx), band, tune);
     const size_t per = plan.per;
     // workspace: 8 GB, or for large orders enough for two resident matrices per SM (one
     // CTA each in k_tridiag), capped at 60 % of the free memory

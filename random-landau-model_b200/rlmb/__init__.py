@@ -34,6 +34,7 @@ _SIGNATURES = {
     "rlmb_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rlmb_get_precision": (ctypes.c_int, [_vp]),
     "rlmb_set_refinement_steps": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "rlmb_set_eigenvalue_pass": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rlmb_heevd_batched": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "rlmb_heevd_host": (ctypes.c_int, [_vp, _c_dp, _c_dp, ctypes.c_int, ctypes.c_int]),
     "rlmb_heevd_batched_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
@@ -230,6 +231,11 @@ class Context:
     def set_refinement_steps(self, steps):
         """Mixed mode: 1 or 2 double-precision refinement steps (default 2)."""
         _check(lib().rlmb_set_refinement_steps(self.h, int(steps)), "rlmb_set_refinement_steps")
+
+    def set_eigenvalue_pass(self, on=True):
+        """Mixed mode, one refinement step: recompute the eigenvalues as Rayleigh quotients of
+        the refined vectors (double-precision eigenvalues for the cost of one residual)."""
+        _check(lib().rlmb_set_eigenvalue_pass(self.h, 1 if on else 0), "rlmb_set_eigenvalue_pass")
 
     def fp64_peak_tflops(self):
         t = ctypes.c_double()
