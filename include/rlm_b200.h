@@ -112,6 +112,10 @@ int rlmb_heev_solver(rlmb_context* ctx, int n, int precision, int* solver);
  * FP64 tensor-core GEMMs).  RLMB_TRIDIAG_AUTO: the built-in choice (divide and conquer from
  * n = 600) or the autotuned one.  Both run in
  * double precision in either precision mode. */
+/* Panel queue of the blocked reduction (orders above 512, chunks of more matrices than SMs; no
+ * counterpart in the reference): CTAs of `threads` = 512 threads, one per SM, or 256 threads,
+ * two per SM, take (matrix, column) units; 0 = the built-in choice. */
+int rlmb_set_panel_queue(rlmb_context* ctx, int n, int precision, int threads);
 #define RLMB_TRIDIAG_AUTO 0
 #define RLMB_TRIDIAG_BISECTION 1
 #define RLMB_TRIDIAG_DC 2

@@ -1390,6 +1390,7 @@ static constexpr int HT_TAIL = 64;   // order below which the unblocked kernel f
 static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
 static constexpr int DC_DEFAULT_MIN = 600;   // orders from which divide and conquer is the built-in tridiagonal solver (measured: even with bisection at 512, 1.4x at 1024, 2.3x at 3000)
 static constexpr int JAC_DEFAULT_MAX = 20;    // orders up to which k_jacobi is the built-in solver (measured: 2.1x the Householder path at 16, even at 24)
+static constexpr int QUEUE_NT_DEFAULT = 512;   // panel queue CTAs: 512 threads, one per SM
 static constexpr int TUNE_MIN_N = 16;         // orders the autotuner tunes: TUNE_MIN_N .. TUNE_MAX_N
 static constexpr int TUNE_MAX_N = 1024;
 
@@ -1612,7 +1613,7 @@ k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double*
 // wait only on earlier claims, which CTAs already running hold: no wait depends on a CTA
 // that has not started.
 template <int NT, class R>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
 k_hetrd_panel_q(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
                 typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ PV,
                 typename Cx<R>::T* __restrict__ PW, int n, int m, int nb, int* q, long long base, int col0,
@@ -2251,6 +2252,7 @@ struct HeevTune {
     int xtile = 0;       // row tile of the double-precision X -= V W' update, 64 or 128
     int bt_nb = 0;       // reflectors per block of the GEMM back-transformation, 64 or 128
     int jacobi = -1;     // 1: batched Jacobi (k_jacobi, orders <= JAC_MAX_N), 0: the Householder path
+    int queue_nt = 0;    // panel queue CTAs: 512 threads (one per SM) or 256 (two per SM); 0: built-in
     int dc = -1;         // tridiagonal stage: 1 divide and conquer (orders <= DC_MAX_N), 0 bisection +
                          // inverse iteration (k_tridiag)
 };
@@ -2276,6 +2278,7 @@ struct HeevPlan {
     int nblk16, bt_nb, nblkbt;   // k_ormtr blocks; GEMM back-transformation block size and count
     int npanels, m_tail;  // blocked reduction: panels of HP_W columns, then k_hetrd on m_tail
     int panel_nt, xtile;  // tuned launch choices (0: built-in)
+    int queue_nt;         // threads of the panel queue's CTAs (512: one per SM, 256: two per SM)
     // per: bytes per matrix of the chunk's regions (offsets off_*, times the chunk size);
     // per2: bytes per matrix of the mixed mode's refinement regions (Res, X1), which the
     // refinement uses for one sub-chunk of matrices at a time
@@ -2288,6 +2291,7 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     HeevPlan p{};
     p.panel_nt = tune.panel_nt;
     p.xtile = tune.xtile;
+    p.queue_nt = tune.queue_nt ? tune.queue_nt : QUEUE_NT_DEFAULT;
     p.n = n;
     p.mixed = mixed;
     p.band = band >= 0 && 32 + 2 * band <= n ? band : -1;   // the band residual needs 32 + 2o <= n
@@ -2407,7 +2411,10 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
             return RLMB_ERR_CUDA;
         // built-in choice above order 512 for chunks of more matrices than SMs: one 512-thread
         // CTA per SM taking (matrix, column) units from a queue (k_hetrd_panel_q)
-        const bool queue = p.panel_nt == 0 && n > 512 && nb > sms && panel_smem<512, R>(n) <= 227 * 1024;
+        const int qnt = p.queue_nt == 256 ? 256 : 512;
+        const int qper = qnt == 256 ? 2 : 1;   // resident queue CTAs per SM
+        const bool queue = p.panel_nt == 0 && n > 512 && nb > sms &&
+                           (qnt == 512 ? panel_smem<512, R>(n) <= 227 * 1024 : panel_smem<256, R>(n) <= 113 * 1024);
         // otherwise one CTA per matrix: 256 threads (two CTAs per SM) for orders 385..512,
         // 512 threads otherwise (measured), unless tuned
         bool mid = n > 384 && n <= 512;
@@ -2415,16 +2422,22 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         if (p.panel_nt == 512) mid = false;
         auto panel = mid ? k_hetrd_panel<256, R> : k_hetrd_panel<512, R>;
         const int pnt = mid ? 256 : 512;
-        const size_t smem = mid ? panel_smem<256, R>(n) : panel_smem<512, R>(n);
-        if (cudaFuncSetAttribute(queue ? (const void*)k_hetrd_panel_q<512, R> : (const void*)panel,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        const size_t smem = queue ? (qnt == 256 ? panel_smem<256, R>(n) : panel_smem<512, R>(n))
+                                  : mid ? panel_smem<256, R>(n) : panel_smem<512, R>(n);
+        const void* qk = qnt == 256 ? (const void*)k_hetrd_panel_q<256, R> : (const void*)k_hetrd_panel_q<512, R>;
+        if (cudaFuncSetAttribute(queue ? qk : (const void*)panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
             return RLMB_ERR_CUDA;
-        const int grid = std::min(nb, sms);
+        const int grid = std::min(nb, queue ? qper * sms : sms);
         // the queue's counters, and its abort flag, which k_panel_abort_info reads in every case
         if (cudaMemsetAsync(Q, 0, (8 + (size_t)nb) * sizeof(int), st) != cudaSuccess) return RLMB_ERR_CUDA;
         for (int k = 0; k < p.npanels; ++k) {
             RLMB_CHUNK_PROF("k_hetrd_panel");
-            if (queue)
+            if (queue && qnt == 256)
+                k_hetrd_panel_q<256, R><<<grid, 256, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, nb, Q,
+                                                                 (long long)k * ((long long)nb * HP_W + grid),
+                                                                 k * HP_W, info);
+            else if (queue)
                 k_hetrd_panel_q<512, R><<<grid, 512, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, nb, Q,
                                                                  (long long)k * ((long long)nb * HP_W + grid),
                                                                  k * HP_W, info);
@@ -3033,9 +3046,10 @@ extern "C" int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int
     auto& tc = tune_cache(ctx);
     auto it = tc.find({n, precision});
     HeevTune t;
-    if (it != tc.end()) {   // the solver choices are set separately
+    if (it != tc.end()) {   // the solver and panel-queue choices are set separately
         t.jacobi = it->second.t.jacobi;
         t.dc = it->second.t.dc;
+        t.queue_nt = it->second.t.queue_nt;
     }
     t.blocked = blocked;
     t.gemm_bt = gemm_bt;
@@ -3056,6 +3070,19 @@ extern "C" int rlmb_set_heev_solver(rlmb_context* ctx, int n, int precision, int
     TuneEntry e{HeevTune{}, 0.0};
     if (it != tc.end()) e = it->second;
     e.t.jacobi = solver == RLMB_SOLVER_AUTO ? -1 : solver == RLMB_SOLVER_JACOBI ? 1 : 0;
+    tc[{n, precision}] = e;
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_set_panel_queue(rlmb_context* ctx, int n, int precision, int threads) {
+    if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED) ||
+        (threads != 0 && threads != 256 && threads != 512))
+        return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
+    TuneEntry e{HeevTune{}, 0.0};
+    if (it != tc.end()) e = it->second;
+    e.t.queue_nt = threads;
     tc[{n, precision}] = e;
     return RLMB_OK;
 }

@@ -45,6 +45,7 @@ _SIGNATURES = {
     "rlmb_set_heev_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "rlmb_heev_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip]),
     "rlmb_set_tridiag_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "rlmb_set_panel_queue": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "rlmb_tridiag_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip]),
     "rlmb_zgemm_batched": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int]),
@@ -302,6 +303,12 @@ class Context:
         n <= 3600), TRIDIAG_BISECTION or TRIDIAG_AUTO (built-in / autotuned)."""
         prec = self.precision if precision is None else precision
         _check(lib().rlmb_set_tridiag_solver(self.h, n, prec, solver), "rlmb_set_tridiag_solver")
+
+    def set_panel_queue(self, n, threads, precision=None):
+        """Pin the panel queue's CTAs for order n: 512 threads (one per SM), 256 (two per SM) or
+        0 (built-in)."""
+        prec = self.precision if precision is None else precision
+        _check(lib().rlmb_set_panel_queue(self.h, n, prec, int(threads)), "rlmb_set_panel_queue")
 
     def tridiag_solver(self, n, precision=None):
         """TRIDIAG_DC or TRIDIAG_BISECTION: the tridiagonal solver order-n eigensolves run with."""

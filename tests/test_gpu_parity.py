@@ -479,12 +479,13 @@ def test_heevd_back_transformation_blocks(n, bs, mixed):
         c.close()
 
 
+@pytest.mark.parametrize("qnt", [512, 256])
 @pytest.mark.parametrize("mixed", [False, True])
-def test_panel_queue_matches_per_matrix_panels(mixed):
-    """A chunk of more matrices than SMs above order 512 runs its panels as one 512-thread CTA
-    per SM taking (matrix, column) units from a queue; it must give the results of the
-    one-CTA-per-matrix kernel of the same width (pinned with panel_threads = 512), and no
-    bounded wait may run out."""
+def test_panel_queue_matches_per_matrix_panels(mixed, qnt):
+    """A chunk of more matrices than SMs above order 512 runs its panels as resident CTAs (512
+    threads one per SM, or 256 threads two per SM) taking (matrix, column) units from a queue;
+    it must give the results of the one-CTA-per-matrix kernel (pinned with panel_threads =
+    512), and no bounded wait may run out."""
     import rlmb
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     n, nb = 576, sms + 13
@@ -498,6 +499,8 @@ def test_panel_queue_matches_per_matrix_panels(mixed):
             if mixed:
                 c.precision = c.MIXED
             c.set_heev_config(n, 1, 1, nt, 0, 0)
+            if nt == 0:
+                c.set_panel_queue(n, qnt)
             a = torch.tensor(np.ascontiguousarray(np.transpose(a0, (0, 2, 1))), device="cuda")
             info = torch.zeros(nb, dtype=torch.int32, device="cuda")
             w = c.heevd(a, info=info)
