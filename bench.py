@@ -975,6 +975,9 @@ def run_probe(args):
     if args.probe == "rlm":
         if args.mixed:
             ctx.precision = ctx.MIXED
+        if args.eigenvalue_pass:
+            ctx.set_refinement_steps(1)
+            ctx.set_eigenvalue_pass(True)
         ctx.rlm_mesh_solve(n, 1.0, 16.0, 4 if n > 1024 else 16, SEED, 0, b)
         torch.cuda.synchronize()
         print(json.dumps({"probe": "rlm", "n": n, "samples": b, "launches": ctx.launches}))
@@ -996,6 +999,9 @@ def run_probe(args):
         return
     if args.mixed:
         ctx.precision = ctx.MIXED
+    if args.eigenvalue_pass:
+        ctx.set_refinement_steps(1)
+        ctx.set_eigenvalue_pass(True)
     if args.solver != "auto":
         ctx.set_heev_solver(n, ctx.SOLVER_JACOBI if args.solver == "jacobi" else ctx.SOLVER_HOUSEHOLDER)
     if args.tridiag != "auto":
@@ -1020,6 +1026,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision measurement on the same inputs")
     ap.add_argument("--mixed", action="store_true", help="probe in the mixed-precision mode")
+    ap.add_argument("--eigenvalue-pass", action="store_true",
+                    help="probes in the mixed mode: one refinement step + the eigenvalue pass")
     ap.add_argument("--probe", default=None, choices=["heevd", "tcgemm", "rlm", "hlm", "fhs"],
                     help="run one small eigensolver batch only (for profiler captures)")
     ap.add_argument("--solver", default="auto", choices=["auto", "householder", "jacobi"],
