@@ -116,6 +116,10 @@ int rlmb_heev_solver(rlmb_context* ctx, int n, int precision, int* solver);
  * counterpart in the reference): CTAs of `threads` = 512 threads, one per SM, or 256 threads,
  * two per SM, take (matrix, column) units; 0 = the built-in choice. */
 int rlmb_set_panel_queue(rlmb_context* ctx, int n, int precision, int threads);
+/* Columns per panel of the blocked reduction: 16 or 32 (rank-32 or rank-64 updates); 0 = the
+ * built-in choice (32 from order 1024 in the FP64 mode, 16 otherwise: in the mixed mode 32
+ * leaves the refinement a larger single-precision error). */
+int rlmb_set_panel_width(rlmb_context* ctx, int n, int precision, int width);
 #define RLMB_TRIDIAG_AUTO 0
 #define RLMB_TRIDIAG_BISECTION 1
 #define RLMB_TRIDIAG_DC 2

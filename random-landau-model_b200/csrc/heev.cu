@@ -1376,16 +1376,23 @@ struct EpSub {     // X(r, c) -= acc
 };
 
 // ------------------------------------------------------------- blocked k_hetrd (large n)
-// For large orders the reduction runs in panels of HP_W columns (LAPACK zlatrd + zher2k,
-// uplo='U', restated): k_hetrd_panel reduces columns m-1 .. m-HP_W of the leading m x m
+// For large orders the reduction runs in panels of pw (16 or 32) columns (LAPACK zlatrd + zher2k,
+// uplo='U', restated): k_hetrd_panel reduces columns m-1 .. m-pw of the leading m x m
 // block one CTA per matrix, keeping each column's reflector v and its w = tau A' v - ...
 // in the panel buffers V, W instead of updating the leading block: column c is first
 // brought up to date with the panel's earlier pairs, its matrix-vector product reads the
 // leading c x c block as stored (read only) and is corrected by the same pairs.  The
-// rank-2*HP_W update A -= V W^H + W V^H of the remaining leading block then runs as a GEMM
+// rank-2*pw update A -= V W^H + W V^H of the remaining leading block then runs as a GEMM
 // over all SMs (launch_zgemm, EpHer2k), and the last block (order <= HT_TAIL) is reduced by
 // k_hetrd.  D, E, TAU and the reflector storage are those of the unblocked reduction.
-static constexpr int HP_W = 16;      // panel width (16 measured faster than 8, 12, 24 and 32 at orders 256-1000)
+// Panel width: in double precision 32 columns from order HP_W_WIDE_MIN (at n = 3000 the
+// rank-64 updates save 17 % of the update time, the panels cost the same), 16 below (measured
+// faster than 8, 12, 24 and 32 at orders 256-1000).  Single precision keeps 16: with 32 the
+// panel folds up to 31 pairs into each column in FP32, and two refinement steps then left an
+// orthogonality defect of 2.6e-10 at n = 1600 (1e-12 with 16), for a 3 % saving.  Shared
+// memory and the pair storage are laid out for the plan's width; HP_W_MAX bounds it.
+static constexpr int HP_W_MAX = 32;
+static constexpr int HP_W_WIDE_MIN = 1024;
 static constexpr int HT_TAIL = 64;   // order below which the unblocked kernel finishes
 static constexpr int HT_BLOCKED_MIN = 256;   // orders from which the blocked reduction runs
 static constexpr int DC_DEFAULT_MIN = 600;   // orders from which divide and conquer is the built-in tridiagonal solver (measured: even with bisection at 512, 1.4x at 1024, 2.3x at 3000)
@@ -1490,7 +1497,7 @@ template <int NT, class R, bool CG>
 __device__ __forceinline__ void panel_column(typename Cx<R>::T* __restrict__ A, double* __restrict__ D,
                                              double* __restrict__ E, typename Cx<R>::T* __restrict__ TAU,
                                              typename Cx<R>::T* __restrict__ PV, typename Cx<R>::T* __restrict__ PW,
-                                             int n, int m, size_t mat, int j, typename Cx<R>::T* vn,
+                                             int n, int m, size_t mat, int j, int pw, typename Cx<R>::T* vn,
                                              typename Cx<R>::T* pn, typename Cx<R>::T* coef, R* red) {
     typedef typename Cx<R>::T C;
     constexpr int NW = NT / 32;
@@ -1499,8 +1506,8 @@ __device__ __forceinline__ void panel_column(typename Cx<R>::T* __restrict__ A, 
     double* dd = D + mat * n;
     double* ee = E + mat * n;
     C* tt = TAU + mat * n;
-    C* V = PV + mat * (size_t)HP_W * n;   // pair q at V + q*n, W + q*n
-    C* W = PW + mat * (size_t)HP_W * n;
+    C* V = PV + mat * (size_t)pw * n;   // pair q at V + q*n, W + q*n
+    C* W = PW + mat * (size_t)pw * n;
     if (m == n && j == 0 && tid == 0) {
         ee[n - 1] = 0.0;
         tt[n - 1] = cz<C>();
@@ -1579,26 +1586,26 @@ __device__ __forceinline__ void panel_column(typename Cx<R>::T* __restrict__ A, 
 }
 
 // Shared work arrays of the panel kernels: vn [m] (column / reflector), pn [m] (A' v
-// accumulator), coef [2*HP_W] (w_q^H v, v_q^H v), red [2*warps].
+// accumulator), coef [2*HP_W_MAX] (w_q^H v, v_q^H v), red [2*warps].
 template <int NT, class R>
 __host__ __device__ constexpr size_t panel_smem(int m) {
-    return (2 * (size_t)m + 2 * HP_W) * sizeof(typename Cx<R>::T) + 2 * (NT / 32) * sizeof(R);
+    return (2 * (size_t)m + 2 * HP_W_MAX) * sizeof(typename Cx<R>::T) + 2 * (NT / 32) * sizeof(R);
 }
 
-// One CTA per matrix: the panel's HP_W columns in order.
+// One CTA per matrix: the panel's pw columns in order.
 template <int NT, class R>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
 k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
               typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ PV,
-              typename Cx<R>::T* __restrict__ PW, int n, int m) {
+              typename Cx<R>::T* __restrict__ PW, int n, int m, int pw) {
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* vn = reinterpret_cast<C*>(smem_raw);
     C* pn = vn + m;
     C* coef = pn + m;
-    R* red = reinterpret_cast<R*>(coef + 2 * HP_W);
-    for (int j = 0; j < HP_W; ++j)
-        panel_column<NT, R, false>(A, D, E, TAU, PV, PW, n, m, blockIdx.x, j, vn, pn, coef, red);
+    R* red = reinterpret_cast<R*>(coef + 2 * HP_W_MAX);
+    for (int j = 0; j < pw; ++j)
+        panel_column<NT, R, false>(A, D, E, TAU, PV, PW, n, m, blockIdx.x, j, pw, vn, pn, coef, red);
 }
 
 // The same panel for chunks of more matrices than SMs: one resident CTA of NT threads per SM
@@ -1609,25 +1616,25 @@ k_hetrd_panel(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double*
 // pair): q[2 + mat] counts the columns of each matrix completed in the chunk; a unit waits
 // for done = col0 + j, a wait bounded by TC_WAIT_NS that sets the abort flag q[1] (and counts
 // in g_tc_fault) when it runs out.  The claims of a launch end with one failed claim per CTA,
-// so launch k's units start at base = k * (nb * HP_W + grid).  Units are claimed in order and
+// so launch k's units start at base = k * (nb * pw + grid).  Units are claimed in order and
 // wait only on earlier claims, which CTAs already running hold: no wait depends on a CTA
 // that has not started.
 template <int NT, class R>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
 k_hetrd_panel_q(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, double* __restrict__ E,
                 typename Cx<R>::T* __restrict__ TAU, typename Cx<R>::T* __restrict__ PV,
-                typename Cx<R>::T* __restrict__ PW, int n, int m, int nb, int* q, long long base, int col0,
+                typename Cx<R>::T* __restrict__ PW, int n, int m, int pw, int nb, int* q, long long base, int col0,
                 int* __restrict__ info) {
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* vn = reinterpret_cast<C*>(smem_raw);
     C* pn = vn + m;
     C* coef = pn + m;
-    R* red = reinterpret_cast<R*>(coef + 2 * HP_W);
+    R* red = reinterpret_cast<R*>(coef + 2 * HP_W_MAX);
     __shared__ long long s_unit;
     __shared__ int s_go;
     const int tid = threadIdx.x;
-    const long long units = (long long)nb * HP_W;
+    const long long units = (long long)nb * pw;
     for (;;) {
         if (tid == 0) {
             long long u = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(q + 4), 1ull) - base;
@@ -1662,7 +1669,7 @@ k_hetrd_panel_q(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, doubl
         if (u >= units || !go) break;
         __threadfence();
         const int mat = (int)(u % nb), j = (int)(u / nb);
-        panel_column<NT, R, true>(A, D, E, TAU, PV, PW, n, m, mat, j, vn, pn, coef, red);
+        panel_column<NT, R, true>(A, D, E, TAU, PV, PW, n, m, mat, j, pw, vn, pn, coef, red);
         // every thread's writes of the column, then the release of the column count
         __threadfence();
         __syncthreads();
@@ -1675,26 +1682,26 @@ k_hetrd_panel_q(typename Cx<R>::T* __restrict__ A, double* __restrict__ D, doubl
 }
 
 // [V | W] (r, k) and [W | V]^H (k, c) of a panel: the operands of A -= V W^H + W V^H.
-template <class C>
+template <class C, int w>
 struct OpPanelA {
     static constexpr bool RFAST = true;
     const C* pv;
     const C* pw;
     int n;
     __device__ __forceinline__ C elem(size_t mat, int r, int k) const {
-        const size_t o = mat * (size_t)HP_W * n;
-        return k < HP_W ? pv[o + (size_t)k * n + r] : pw[o + (size_t)(k - HP_W) * n + r];
+        const size_t o = mat * (size_t)w * n;
+        return k < w ? pv[o + (size_t)k * n + r] : pw[o + (size_t)(k - w) * n + r];
     }
 };
-template <class C>
+template <class C, int w>
 struct OpPanelB {
     static constexpr bool KFAST = false;
     const C* pv;
     const C* pw;
     int n;
     __device__ __forceinline__ C elem(size_t mat, int k, int c) const {
-        const size_t o = mat * (size_t)HP_W * n;
-        return cconj(k < HP_W ? pw[o + (size_t)k * n + c] : pv[o + (size_t)(k - HP_W) * n + c]);
+        const size_t o = mat * (size_t)w * n;
+        return cconj(k < w ? pw[o + (size_t)k * n + c] : pv[o + (size_t)(k - w) * n + c]);
     }
 };
 // A(r, c) -= acc on and above the diagonal (real diagonal); tiles below it are skipped.
@@ -2253,6 +2260,7 @@ struct HeevTune {
     int bt_nb = 0;       // reflectors per block of the GEMM back-transformation, 64 or 128
     int jacobi = -1;     // 1: batched Jacobi (k_jacobi, orders <= JAC_MAX_N), 0: the Householder path
     int queue_nt = 0;    // panel queue CTAs: 512 threads (one per SM) or 256 (two per SM); 0: built-in
+    int panel_w = 0;     // panel width, 16 or 32; 0: built-in (32 from order HP_W_WIDE_MIN in FP64)
     int dc = -1;         // tridiagonal stage: 1 divide and conquer (orders <= DC_MAX_N), 0 bisection +
                          // inverse iteration (k_tridiag)
 };
@@ -2276,7 +2284,8 @@ struct HeevPlan {
     int ch, dbuf;
     size_t smem_orm;
     int nblk16, bt_nb, nblkbt;   // k_ormtr blocks; GEMM back-transformation block size and count
-    int npanels, m_tail;  // blocked reduction: panels of HP_W columns, then k_hetrd on m_tail
+    int npanels, m_tail;  // blocked reduction: panels of pw columns, then k_hetrd on m_tail
+    int pw;               // panel width, 16 or 32
     int panel_nt, xtile;  // tuned launch choices (0: built-in)
     int queue_nt;         // threads of the panel queue's CTAs (512: one per SM, 256: two per SM)
     // per: bytes per matrix of the chunk's regions (offsets off_*, times the chunk size);
@@ -2305,9 +2314,10 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
         return p;
     }
     const size_t ce = mixed ? sizeof(cplxf) : sizeof(cplx);   // working complex element
-    const bool blocked = tune.blocked < 0 ? n >= HT_BLOCKED_MIN : (tune.blocked > 0 && n > HT_TAIL + HP_W);
-    p.npanels = blocked ? (n - HT_TAIL + HP_W - 1) / HP_W : 0;
-    p.m_tail = n - p.npanels * HP_W;
+    p.pw = tune.panel_w ? tune.panel_w : n >= HP_W_WIDE_MIN && !mixed ? 32 : 16;
+    const bool blocked = tune.blocked < 0 ? n >= HT_BLOCKED_MIN : (tune.blocked > 0 && n > HT_TAIL + p.pw);
+    p.npanels = blocked ? (n - HT_TAIL + p.pw - 1) / p.pw : 0;
+    p.m_tail = n - p.npanels * p.pw;
     p.hc = mixed ? hetrd_config<float>(p.m_tail) : hetrd_config<double>(p.m_tail);
     p.smem_tri = 4 * (size_t)n * sizeof(double) + n * sizeof(int);
     p.nblk16 = (n - 1 + ORM_NB - 1) / ORM_NB;
@@ -2350,7 +2360,7 @@ static HeevPlan heev_plan(int n, bool mixed, int refine_steps = 2, int band = -1
     p.off_y = off; off += mixed ? r256((size_t)n * RF_KMAX * sizeof(cplx)) : 0;
     p.off_mu = off; off += mixed ? r256(n * sizeof(double)) : 0;
     p.off_st = off; off += mixed ? r256(3 * (size_t)n * sizeof(double)) : 0;
-    p.off_pv = off; off += p.npanels > 0 ? r256(2 * (size_t)HP_W * n * ce) : 0;   // panel V, W
+    p.off_pv = off; off += p.npanels > 0 ? r256(2 * (size_t)p.pw * n * ce) : 0;   // panel V, W
     p.off_q = off; off += p.npanels > 0 ? r256(16) : 0;   // panel queue: claims, abort flag, column counts
     p.per = off;
     p.per2 = mixed ? r256(nn * sizeof(cplx)) : 0;                              // residual R
@@ -2395,7 +2405,7 @@ size_t heev_max_chunk(int n) {
     } while (0)
 
 // Householder tridiagonalisation in the working precision R: blocked panels (k_hetrd_panel +
-// rank-2*HP_W GEMM update) down to order m_tail, then k_hetrd on the leading block.  PV holds
+// rank-2*pw GEMM update) down to order m_tail, then k_hetrd on the leading block.  PV holds
 // the panel pairs of the chunk (V of every matrix, then W of every matrix).
 template <class R>
 static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p, int nb, typename Cx<R>::T* A,
@@ -2405,7 +2415,8 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
     const int n = p.n;
     int m = n;
     if (p.npanels > 0) {
-        C* PWb = PV + (size_t)nb * HP_W * n;
+        const int pw = p.pw;
+        C* PWb = PV + (size_t)nb * pw * n;
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
             return RLMB_ERR_CUDA;
@@ -2434,20 +2445,25 @@ static int tridiagonalise(rlmb_context* ctx, cudaStream_t st, const HeevPlan& p,
         for (int k = 0; k < p.npanels; ++k) {
             RLMB_CHUNK_PROF("k_hetrd_panel");
             if (queue && qnt == 256)
-                k_hetrd_panel_q<256, R><<<grid, 256, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, nb, Q,
-                                                                 (long long)k * ((long long)nb * HP_W + grid),
-                                                                 k * HP_W, info);
+                k_hetrd_panel_q<256, R><<<grid, 256, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, pw, nb, Q,
+                                                                 (long long)k * ((long long)nb * pw + grid),
+                                                                 k * pw, info);
             else if (queue)
-                k_hetrd_panel_q<512, R><<<grid, 512, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, nb, Q,
-                                                                 (long long)k * ((long long)nb * HP_W + grid),
-                                                                 k * HP_W, info);
+                k_hetrd_panel_q<512, R><<<grid, 512, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, pw, nb, Q,
+                                                                 (long long)k * ((long long)nb * pw + grid),
+                                                                 k * pw, info);
             else
-                panel<<<nb, pnt, smem, st>>>(A, D, E, TAU, PV, PWb, n, m);
+                panel<<<nb, pnt, smem, st>>>(A, D, E, TAU, PV, PWb, n, m, pw);
             RLMB_CHUNK_LAUNCHED();
-            m -= HP_W;
+            m -= pw;
             RLMB_CHUNK_PROF("k_hetrd_her2k");
-            if (launch_work_gemm<C, 64>(st, OpPanelA<C>{PV, PWb, n}, OpPanelB<C>{PV, PWb, n}, EpHer2k<C>{A, n}, m, m,
-                                    2 * HP_W, nb) != cudaSuccess)
+            // (the width a compile-time constant of the operands: their loads are the tile's work)
+            const cudaError_t eu =
+                pw == 32 ? launch_work_gemm<C, 64>(st, OpPanelA<C, 32>{PV, PWb, n}, OpPanelB<C, 32>{PV, PWb, n},
+                                                   EpHer2k<C>{A, n}, m, m, 64, nb)
+                         : launch_work_gemm<C, 64>(st, OpPanelA<C, 16>{PV, PWb, n}, OpPanelB<C, 16>{PV, PWb, n},
+                                                   EpHer2k<C>{A, n}, m, m, 32, nb);
+            if (eu != cudaSuccess)
                 return RLMB_ERR_CUDA;
             RLMB_CHUNK_LAUNCHED();
         }
@@ -3050,6 +3066,7 @@ extern "C" int rlmb_set_heev_config(rlmb_context* ctx, int n, int precision, int
         t.jacobi = it->second.t.jacobi;
         t.dc = it->second.t.dc;
         t.queue_nt = it->second.t.queue_nt;
+        t.panel_w = it->second.t.panel_w;
     }
     t.blocked = blocked;
     t.gemm_bt = gemm_bt;
@@ -3083,6 +3100,19 @@ extern "C" int rlmb_set_panel_queue(rlmb_context* ctx, int n, int precision, int
     TuneEntry e{HeevTune{}, 0.0};
     if (it != tc.end()) e = it->second;
     e.t.queue_nt = threads;
+    tc[{n, precision}] = e;
+    return RLMB_OK;
+}
+
+extern "C" int rlmb_set_panel_width(rlmb_context* ctx, int n, int precision, int width) {
+    if (!ctx || n <= 0 || (precision != RLMB_PRECISION_FP64 && precision != RLMB_PRECISION_MIXED) ||
+        (width != 0 && width != 16 && width != 32))
+        return RLMB_ERR_ARG;
+    auto& tc = tune_cache(ctx);
+    auto it = tc.find({n, precision});
+    TuneEntry e{HeevTune{}, 0.0};
+    if (it != tc.end()) e = it->second;
+    e.t.panel_w = width;
     tc[{n, precision}] = e;
     return RLMB_OK;
 }

@@ -46,6 +46,7 @@ _SIGNATURES = {
     "rlmb_heev_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip]),
     "rlmb_set_tridiag_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "rlmb_set_panel_queue": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "rlmb_set_panel_width": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "rlmb_tridiag_solver": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_ip]),
     "rlmb_zgemm_batched": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int]),
@@ -309,6 +310,11 @@ class Context:
         0 (built-in)."""
         prec = self.precision if precision is None else precision
         _check(lib().rlmb_set_panel_queue(self.h, n, prec, int(threads)), "rlmb_set_panel_queue")
+
+    def set_panel_width(self, n, width, precision=None):
+        """Pin the blocked reduction's panel width for order n: 16, 32 or 0 (built-in)."""
+        prec = self.precision if precision is None else precision
+        _check(lib().rlmb_set_panel_width(self.h, n, prec, int(width)), "rlmb_set_panel_width")
 
     def tridiag_solver(self, n, precision=None):
         """TRIDIAG_DC or TRIDIAG_BISECTION: the tridiagonal solver order-n eigensolves run with."""

@@ -540,3 +540,33 @@ def test_heevd_autotune_picks_and_caches():
             assert np.abs(w2[0] - w[0]).max() <= 1e-12 * np.abs(w[0]).max()
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("n,width,mixed", [(300, 32, False), (700, 32, False), (1537, 16, False),
+                                           (1100, 0, False), (1537, 16, True), (1100, 0, True), (700, 32, True)])
+def test_heevd_panel_widths(n, width, mixed):
+    """Panels of 16 and 32 columns (rank-32 / rank-64 updates) at orders where they are not the
+    built-in width (0 = built-in: 32 from order 1024 in FP64, 16 in the mixed mode); the mixed
+    mode's bound or FP64's, except the orthogonality of the mixed mode, 1e-9: at orders around
+    1500, two refinement steps leave defects of 1e-10 .. 3e-10 (Frobenius norm over n^2 entries)
+    on some random matrices, with either width."""
+    import rlmb
+    c = rlmb.Context(0)
+    try:
+        if mixed:
+            c.precision = c.MIXED
+        c.set_panel_width(n, width)
+        rng = np.random.default_rng(n + width)
+        mats = [_hermitian(rng, n) for _ in range(2)]
+        w, X = _run_heevd(c, mats)
+        tol = 1e-10 if mixed else 1e-12
+        for b, M in enumerate(mats):
+            wref = np.linalg.eigvalsh(M)
+            assert np.abs(w[b] - wref).max() <= tol * np.abs(wref).max()
+            assert np.linalg.norm(M @ X[b] - X[b] * w[b][None, :]) <= (tol if mixed else 2e-15 * n) * np.linalg.norm(M)
+            orth = 1e-9 if mixed else 2e-14 * n
+            assert np.linalg.norm(X[b].conj().T @ X[b] - np.eye(n)) <= orth
+        with pytest.raises(rlmb.RlmbError):
+            c.set_panel_width(n, 24)
+    finally:
+        c.close()
