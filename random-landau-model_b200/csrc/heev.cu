@@ -6,8 +6,9 @@
 // calls reach is restated from its published algorithms:
 //
 //   reduction      A = Q T Q^H (zhetrd, uplo='U').  From order 256: panels of 16 columns
-//                  (k_hetrd_panel, zlatrd restated, one CTA per matrix) whose rank-32
-//                  updates run as batched GEMMs over all SMs (launch_zgemm); the last leading
+//                  (32 from order 1024 in double precision; k_hetrd_panel, zlatrd restated)
+//                  whose rank-32 (rank-64) updates run as batched GEMMs over all SMs
+//                  (launch_zgemm); the last leading
 //                  block (order <= 64, or all of a smaller matrix) by the unblocked,
 //                  look-ahead k_hetrd (zhetd2), its triangle resident in shared memory.
 //   tridiagonal    below order 600 k_tridiag: eigenvalues by Sturm counts (dstebz restated,
