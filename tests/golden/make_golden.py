@@ -47,8 +47,9 @@ def hlm_lib():
     return lib
 
 
-def rlm_reference(n_phi, qc, ic, g, n_sample, seed, threads=8, keep_kpoints=()):
-    """Per-sample loop of rlm/main_rlm_cpu.cpp:109-243 over the reference's functions."""
+def rlm_reference(n_phi, qc, ic, g, n_sample, seed, threads=8, keep_kpoints=(), first=0):
+    """Per-sample loop of rlm/main_rlm_cpu.cpp:109-243 over the reference's functions, for
+    samples first .. n_sample - 1 (each sample's disorder is its own draw of the seeded stream)."""
     lib = rlm_lib()
     L1 = L2 = math.sqrt(n_phi * qc)
     n_imp = int(ic * n_phi / qc)
@@ -63,7 +64,7 @@ def rlm_reference(n_phi, qc, ic, g, n_sample, seed, threads=8, keep_kpoints=()):
                impurity_num=n_imp, off_head=o, coeff_mn=cmn, coeff_m_theta=cmt, coeff_jm=cjm)
     E_all, C_all, Craw_all, emesh, x_all, y_all, s_all, v_all, lines_all = [], [], [], [], [], [], [], [], []
     kp = {}
-    for n in range(n_sample):
+    for n in range(first, n_sample):
         x = np.zeros(n_imp)
         y = np.zeros(n_imp)
         s = np.zeros(n_imp)
@@ -200,6 +201,21 @@ def full_size(which):
                             **{k: v for k, v in r.items() if k in keep})
 
 
+def rlm_n3000_samples(first, last, threads=8):
+    """rlm n_phi = 3000, g = 4, seed 1: samples first .. last (the rest of the headline bench
+    step, whose sample 0 is rlm_n3000_g4_c1_s1_full.npz), one file per sample so that the run can
+    be split and resumed."""
+    keep = ("n_phi", "qc", "ic", "n_mesh", "n_sample", "seed", "impurity_num", "off_head",
+            "energies", "chern", "chern_raw")
+    for smp in range(first, last + 1):
+        path = os.path.join(HERE, f"rlm_n3000_g4_s1_sample{smp}.npz")
+        if os.path.exists(path):
+            continue
+        r = rlm_reference(3000, 1.0, 16.0, 4, smp + 1, 1, threads=threads, first=smp)
+        r["sample"] = np.array(smp)
+        np.savez_compressed(path, sample=r["sample"], **{k: v for k, v in r.items() if k in keep})
+
+
 def run_program(args, workdir):
     env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
     subprocess.run(args, cwd=workdir, env=env, check=True, capture_output=True)
@@ -255,7 +271,9 @@ def main():
 
 
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "--full":
+    if len(sys.argv) > 1 and sys.argv[1] == "--n3000-samples":   # --n3000-samples FIRST LAST
+        rlm_n3000_samples(int(sys.argv[2]), int(sys.argv[3]))
+    elif len(sys.argv) > 1 and sys.argv[1] == "--full":
         for w in sys.argv[2:] or ["hlm", "rlm", "n3000"]:
             full_size(w)
     else:

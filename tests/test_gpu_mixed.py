@@ -323,3 +323,22 @@ def test_mixed_eigenvalue_pass_needs_one_step(ctx):
     # not bit-reproducible from call to call)
     assert np.abs(np.asarray(w2) - np.asarray(w2p)).max() <= 1e-13 * np.abs(np.asarray(w2)).max()
     assert rlmb.lib().rlmb_set_eigenvalue_pass(None, 1) == -1
+
+
+def test_mixed_eigenvalue_pass_bench_step_samples(ctx):
+    """The headline mixed variant (one step + eigenvalue pass) on samples 1 .. 7 of the
+    n_phi = 3000 bench step, against the reference: energies within 1e-10, Chern integers
+    identical (raw values within 1e-3, see test_mixed_eigenvalue_pass_benchmark_geometries)."""
+    fx = {k: os.path.join(GOLDEN, f"rlm_n3000_g4_s1_sample{k}.npz") for k in range(1, 8)
+          if os.path.exists(os.path.join(GOLDEN, f"rlm_n3000_g4_s1_sample{k}.npz"))}
+    if not fx:
+        pytest.skip("no n_phi = 3000 sample fixtures generated")
+    lo, hi = min(fx), max(fx)
+    with _OneStepRQ(ctx):
+        e, c = ctx.rlm_mesh_solve(3000, 1.0, 16.0, 4, 1, lo, hi - lo + 1)
+    for k, path in fx.items():
+        d = np.load(path)
+        eref, cref = d["energies"][0], d["chern"][0]
+        assert np.abs(e[k - lo] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[k - lo]), np.rint(cref))
+        assert np.abs(c[k - lo] - cref).max() < 1e-3

@@ -570,3 +570,27 @@ def test_heevd_panel_widths(n, width, mixed):
             c.set_panel_width(n, 24)
     finally:
         c.close()
+
+
+def _n3000_sample_fixtures():
+    import os
+    from conftest import GOLDEN
+    return {k: os.path.join(GOLDEN, f"rlm_n3000_g4_s1_sample{k}.npz") for k in range(1, 8)
+            if os.path.exists(os.path.join(GOLDEN, f"rlm_n3000_g4_s1_sample{k}.npz"))}
+
+
+def test_rlm_3000_bench_step_samples(ctx):
+    """rlm n_phi = 3000, g = 4, seed 1: the other samples of the headline bench step (1 .. 7,
+    one reference file each) solved in one call, against the reference."""
+    fx = _n3000_sample_fixtures()
+    if not fx:
+        pytest.skip("no n_phi = 3000 sample fixtures generated")
+    lo, hi = min(fx), max(fx)
+    e, c = ctx.rlm_mesh_solve(3000, 1.0, 16.0, 4, 1, lo, hi - lo + 1)
+    assert ctx.last_failures == 0
+    for k, path in fx.items():
+        d = np.load(path)
+        eref, cref = d["energies"][0], d["chern"][0]
+        assert np.abs(e[k - lo] - eref).max() <= 1e-10 * np.abs(eref).max()
+        assert np.array_equal(np.rint(c[k - lo]), np.rint(cref))
+        assert np.abs(c[k - lo] - cref).max() < 1e-8
